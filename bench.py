@@ -1,0 +1,300 @@
+#!/usr/bin/env python
+"""DOF-updates/s of the ZuikakuCFD per-step compute on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--no-cpu-baseline]
+
+One "step" is one SSP-RK3 step (updateMesh) over the whole grid of the
+workload, inputs resident in HBM.  value = DOF-updates/s of the whole job
+(cell updates x DOFs per cell, summed over ranks; each rank owns an
+independent seeded problem: weak scaling, no data-path collective).  rank 0
+prints one JSON line.  Timing: CUDA events on the library's stream around
+exactly K steps, barrier + synchronize on both sides, max over ranks.
+
+--impl reference times the reference's own CPU implementation (its sources
+built unmodified as oracle/_ref, x-slab threads standing in for MPI ranks) on
+a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DOF-updates/s on 1 B200: mixed-prec+learned limiter vs plain FP64 at equal L1"
+UNIT = "DOF-updates/s"
+
+# Algorithmic work per updated cell per RK stage (face-deduplicated, 1 flop per
+# add/sub/mul/div/sqrt/min/max; derivation in DESIGN.md).
+WENO_FLOPS_PER_CELL_STAGE = 1330.0
+
+
+def make_workload(name: str, rank: int):
+    from zuikakucfd_b200 import cases
+    seed = 1000 + rank
+    if name == "weno_jet_2048x1024":
+        c = cases.high_mach_jet(2048, 1024)
+        dt = 0.4 * c.da / (30.0 + float(np.sqrt(c.gamma * 0.4127 / 5.0)))
+        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=dt,
+                    desc="high-Mach jet 2048x1024 (rho=5,u=30 band, gamma=5/3), WENO5+HLLC+SSP-RK3")
+    if name == "weno_fq_2048":
+        c = cases.four_quadrant(2048, seed=seed)
+        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.5),
+                    desc="seeded four-quadrant Riemann 2048x2048, WENO5+HLLC+SSP-RK3, CFL 0.5")
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def allreduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def measure_peaks(device: int) -> dict:
+    import ctypes as C
+    from zuikakucfd_b200 import _native as N
+    out = {}
+    for kind, name in ((0, "fp64_tflops"), (1, "fp32_tflops")):
+        v = C.c_double()
+        N.check(N.lib().zk_peak_flops(device, kind, C.byref(v)))
+        out[name] = v.value
+    return out
+
+
+def cpu_baseline(w: dict, seconds: float = 15.0) -> dict:
+    """The reference's own sources (oracle/_ref, Makefile flags) on this host's
+    cores: x-slab threads standing in for MPI ranks, a bounded sample."""
+    from oracle.oracle import Reference, reference_available
+    if not reference_available("faithful"):
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    c = w["case"]
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    R = Reference("faithful")
+    U = c.conserved()
+    # calibrate on one step, then run enough steps for ~`seconds` of work
+    ms, cells = R.weno_slabs_timed(U, c.bctype, c.da, c.gamma, w["dt"], 1, cores)
+    n = max(1, int(seconds * 1e3 / max(ms, 1.0)))
+    ms, cells = R.weno_slabs_timed(U, c.bctype, c.da, c.gamma, w["dt"], n, cores)
+    v = cells * w["dof_per_cell"] * n / (ms * 1e-3)
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{n} x updateMesh on the full {c.ny}x{c.nx} grid split into {cores} x-slabs "
+                      f"(one thread per slab, reference Makefile flags, halo exchange omitted)",
+            "ms": ms}
+
+
+def run_reference_arm(args, w) -> dict:
+    from oracle.oracle import Reference, reference_available
+    if not reference_available("faithful"):
+        return {"impl": "reference", "unavailable": "oracle/_ref (reference built from its sources) missing"}
+    c = w["case"]
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    R = Reference("faithful")
+    U = c.conserved()
+    # bounded sample: a horizontal strip of the grid sized for <= ~1.5 s per step
+    ms1, _ = R.weno_slabs_timed(U[:, :256], c.bctype[:256], c.da, c.gamma, w["dt"], 1, cores)
+    rows = int(min(c.ny, max(64, 256 * 1500.0 / max(ms1, 1.0))))
+    Us, bs = np.ascontiguousarray(U[:, :rows]), np.ascontiguousarray(c.bctype[:rows]).copy()
+    bs[-3:] = -1
+    for _ in range(args.warmup):
+        R.weno_slabs_timed(Us, bs, c.da, c.gamma, w["dt"], 1, cores)
+    ms, cells = R.weno_slabs_timed(Us, bs, c.da, c.gamma, w["dt"], args.steps, cores)
+    v = cells * w["dof_per_cell"] * args.steps / (ms * 1e-3)
+    sample = (f"{rows}x{c.nx} strip of the {c.ny}x{c.nx} grid per step, {cores} x-slab threads, "
+              f"reference Makefile flags")
+    return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "grid": [c.ny, c.nx]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="weno_jet_2048x1024")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args, make_workload(args.workload, 0))), flush=True)
+        return
+
+    from zuikakucfd_b200 import Solver
+    w = make_workload(args.workload, rank)
+    c = w["case"]
+    s = Solver(method=w["method"], order=max(w["order"], 1), precision="fp64", device=local)
+    s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
+    U0 = c.conserved() if w["method"] == "weno" else c.dg_state(w["order"])
+    s.set_state(U0)
+    cells = c.fluid_cells
+    dofs = cells * w["dof_per_cell"]
+
+    for _ in range(args.warmup):
+        s.step(w["dt"], 1)
+    s.synchronize()
+    barrier(pg)
+    with ClockSampler(local) as clk:
+        ms = s.step_timed(w["dt"], args.steps)  # CUDA events on the library stream
+        s.synchronize()
+    barrier(pg)
+    ms_max = allreduce_max(pg, ms)
+    status = s.status_word()
+    value = world * dofs * args.steps / (ms_max * 1e-3)
+
+    # end to end through the public API with host buffers: the reference
+    # driver's loop (computeMaxSpeed -> dt on the host -> updateMesh), state
+    # uploaded from pinned host memory at the start and read back at the end
+    import torch
+    host_in = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    state_bytes = host_in.numel() * 8
+    barrier(pg)
+    t0 = time.perf_counter()
+    import ctypes as C
+    from zuikakucfd_b200 import _native as N
+    L = N.lib()
+    N.check(L.zk_set_state(s._h, C.cast(host_in.data_ptr(), C.POINTER(C.c_double))))
+    lam = C.c_double()
+    for _ in range(args.steps):
+        N.check(L.zk_max_speed(s._h, C.byref(lam)))
+        N.check(L.zk_step(s._h, C.c_double(w["dt"]), 1))
+    N.check(L.zk_get_state(s._h, C.cast(host_out.data_ptr(), C.POINTER(C.c_double))))
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0)
+    e2e = {"value": world * dofs * args.steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": state_bytes / args.steps + 8,
+           "d2h_bytes_per_step": state_bytes / args.steps + 8,
+           "what": "reference driver loop per step: zk_max_speed (8 B read back) + zk_step(dt); "
+                   "state H2D from pinned host at start, D2H at end, amortised per step"}
+
+    out = None
+    if rank == 0:
+        peaks = measure_peaks(local)
+        stage_ms = ms / (3 * args.steps)  # every launch in the timed region is the stage kernel
+        flops = cells * WENO_FLOPS_PER_CELL_STAGE
+        achieved = flops / (stage_ms * 1e-3) / 1e12
+        hbm_bytes = cells * 97.0  # FP64 state in + U^n + out + kind byte, per stage (avg of 65/97/97)
+        peaks_file = ROOT / "MEASURED_PEAKS.json"
+        hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
+        roof = {"bound": "fp64", "achieved": achieved, "peak": peaks["fp64_tflops"], "unit": "TFLOP/s",
+                "frac": achieved / peaks["fp64_tflops"], "traffic": None,
+                "kernel": "weno_stage_fp64_kernel", "avg_launch_ms": stage_ms,
+                "peak_source": "measured: zk_peak_flops FP64 FMA microbenchmark (MEASURED_PEAKS.json has no FP64 figure)",
+                "hbm": {"achieved_gbs": hbm_bytes / (stage_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak}}
+        cpu = {"value": None, "skipped": True} if args.no_cpu_baseline or world > 1 else cpu_baseline(w)
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+               "config": {"workload": args.workload, "desc": w["desc"], "grid": [c.ny, c.nx],
+                          "updated_cells": cells, "dof_per_cell": w["dof_per_cell"], "precision": "fp64",
+                          "l2": "working set (3 FP64 states = %.0f MB) larger than the 126 MB L2" %
+                                (3 * state_bytes / 1e6),
+                          "parallelism": f"replicas x{world} (independent seeded problems)"},
+               "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 3 * args.steps,
+               "roofline": roof, "cpu_baseline": cpu, "status_word": status, "peaks": peaks}
+        print(json.dumps(out), flush=True)
+    s.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+/* zuikaku.h -- C ABI of the B200 (sm_100a) per-step compute for ZuikakuCFD's
+ * explicit 2D Euler solvers: WENO5 finite volume and DG P=1..3, SSP-RK3, the
+ * DG limiters and the CFL max-wavespeed reduction.
+ *
+ * Every entry point returns an int status (ZK_OK = 0) and never throws.  A
+ * context owns its device state and one CUDA stream; it is externally
+ * synchronised (one host thread at a time).  zk_last_error() gives the message
+ * of the last failure on the calling thread.
+ *
+ * Host arrays at this boundary are row-major planes, row i = y index (row 0 on
+ * top, as in the reference's .dat files), column j = x:
+ *   WENO state   double U[4][ny][nx]          rho, rho*u, rho*v, E
+ *   DG state     double dof[4][NM][ny][nx]    NM = (P+1)^2, mode m = px*(P+1)+py
+ *   bctype       int32 [ny][nx]               0 fluid, -1 copy ghost, 1 slip
+ *                                             wall (DG), -3 exchange ghost
+ * The reference stores the same fields as column-major Eigen matrices
+ * (src_WENO/fluid.h:26-80, src_DG/fluid.h:44-110); src_WENO/fluid.cpp:391-393
+ * gives its index map idx(i,j) = j*ny + i.
+ */
+#ifndef ZUIKAKU_H
+#define ZUIKAKU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+    ZK_OK = 0,
+    ZK_ERR_ARG = 1,       /* invalid argument (null pointer, bad size, bad option) */
+    ZK_ERR_STATE = 2,     /* call out of order (no mesh set, ...)                  */
+    ZK_ERR_CUDA = 3,      /* a CUDA runtime call failed                            */
+    ZK_ERR_NUMERIC = 4,   /* the device status word reported NaN / non-positive    */
+    ZK_ERR_UNSUPPORTED = 5,
+    ZK_ERR_IO = 6,
+    ZK_ERR_TIMEOUT = 7
+};
+
+/* ---- options -------------------------------------------------------------- */
+enum { ZK_METHOD_WENO = 0, ZK_METHOD_DG = 1 };
+/* FP64: the reference's arithmetic op for op (bit-identical to the reference
+ * built with -ffp-contract=off).  MIXED: FP32 reconstruction/fluxes/quadrature
+ * with FP64 conserved-state accumulation and FP64 pressure recovery. */
+enum { ZK_PREC_FP64 = 0, ZK_PREC_MIXED = 1 };
+/* DG limiter: REFERENCE = Persson modal filter + Zhang-Shu positivity
+ * (src_DG/fluid.cpp:824-992); NONE; TVB = Cockburn-Shu TVB minmod (M) with
+ * characteristic limiting; TVB_MLP = TVB limiting of the cells a learned
+ * indicator flags. */
+enum { ZK_LIMITER_REFERENCE = 0, ZK_LIMITER_NONE = 1, ZK_LIMITER_TVB = 2, ZK_LIMITER_TVB_MLP = 3 };
+enum { ZK_FLUX_HLLC = 0, ZK_FLUX_HLL = 1 };
+/* Boundary handling of bctype -3 cells: EXCHANGE leaves them alone (the
+ * reference at one rank); PERIODIC refills them with their periodic image
+ * inside the 3-wide ring before every RHS evaluation. */
+enum { ZK_BOUNDARY_EXCHANGE = 0, ZK_BOUNDARY_PERIODIC = 1 };
+
+typedef struct zk_options {
+    int method;     /* ZK_METHOD_*                           */
+    int order;      /* DG polynomial degree P in 1..3        */
+    int precision;  /* ZK_PREC_*                             */
+    int limiter;    /* ZK_LIMITER_* (DG only)                */
+    int flux;       /* ZK_FLUX_* (DG only; WENO is HLLC)     */
+    int boundary;   /* ZK_BOUNDARY_*                         */
+    int device;     /* CUDA device ordinal                   */
+    double tvb_M;   /* TVB constant M (default 50)           */
+} zk_options;
+
+typedef struct zk_ctx zk_ctx;
+
+/* Fills *opt with defaults: WENO, P=2, FP64, reference limiter, HLLC,
+ * exchange boundary, device 0, M=50. */
+void zk_default_options(zk_options* opt);
+
+int zk_create(const zk_options* opt, zk_ctx** out);
+int zk_destroy(zk_ctx* ctx);
+const char* zk_last_error(void);
+int zk_version(void);
+
+/* Grid and boundary codes; allocates the device state.  Replaces the sizing
+ * part of Mesh(folder) (src_WENO/fluid.cpp:68-94, src_DG/fluid.cpp:216-244). */
+int zk_set_mesh(zk_ctx* ctx, int ny, int nx, double da, double gamma, const int32_t* bctype);
+
+/* Host <-> device state (layouts above).  The state stays device-resident
+ * between steps; these are the only host copies the step loop needs. */
+int zk_set_state(zk_ctx* ctx, const double* host_state);
+int zk_get_state(zk_ctx* ctx, double* host_state);
+/* Number of doubles in the host state (4*ny*nx or 4*NM*ny*nx). */
+size_t zk_state_size(const zk_ctx* ctx);
+
+/* Mesh(folder): read params.txt + rho/u/v/p/bctype.dat, convert to conserved
+ * variables and, for DG, initialise mode 0 (src_DG/fluid.cpp:173-182). */
+int zk_load_case(zk_ctx* ctx, const char* dir);
+
+/* updateMesh x nsteps: one SSP-RK3 step each (src_WENO/fluid.cpp:468-493,
+ * src_DG/fluid.cpp:1005-1054), ghost fill and limiter included, fixed dt. */
+int zk_step(zk_ctx* ctx, double dt, int nsteps);
+
+/* computeRHS (src_WENO/fluid.cpp:328-463 / src_DG/fluid.cpp:656-807): fills
+ * the ghosts of the device state in place, as the reference mutates its Mesh,
+ * and writes dU to host memory.  WENO dU includes dt; DG dU = d(dof)/dt. */
+int zk_rhs(zk_ctx* ctx, double dt, double* host_dU);
+
+/* applyLimiter (src_DG/fluid.cpp:824-992) on the device state (DG only). */
+int zk_limit(zk_ctx* ctx);
+
+/* Max wave speed: WENO computeMaxSpeed (src_WENO/fluid.cpp:539-553, all
+ * cells); DG computeMaxSpeedDG_omp (src_DG/solver.cpp:26-64, fluid cells,
+ * 4 corners). */
+int zk_max_speed(zk_ctx* ctx, double* out);
+
+/* recoverPrimitives (src_WENO/fluid.cpp:500-515): prim[4][ny][nx] =
+ * rho, u, v, p of the cell averages, FP64. */
+int zk_recover_primitives(zk_ctx* ctx, double* host_prim);
+
+/* Device status word (bit 0: NaN seen, bit 1: rho <= 0, bit 2: p <= 0) of the
+ * last zk_step; cleared by each zk_step. */
+int zk_status_word(zk_ctx* ctx, uint32_t* out);
+
+/* Stream control: run on an external stream (e.g. one owned by a framework)
+ * instead of the context's own; NULL restores the context stream. */
+int zk_set_stream(zk_ctx* ctx, void* cuda_stream);
+int zk_synchronize(zk_ctx* ctx);
+
+/* Timing helper: runs nsteps steps and returns the device time measured with
+ * CUDA events on the context's stream. */
+int zk_step_timed(zk_ctx* ctx, double dt, int nsteps, float* ms);
+
+/* Device pointer of the FP64 state (layout: planes of ny rows x pitch
+ * doubles) and its row pitch in elements, for zero-copy callers. */
+int zk_state_device(zk_ctx* ctx, double** dptr, int* pitch);
+
+/* FMA-throughput microbenchmark of one device: kind 0 = FP64, 1 = FP32;
+ * writes the achieved dense TFLOP/s (2 flops per FMA).  Roofline denominator
+ * for kernels bound by the FP pipes. */
+int zk_peak_flops(int device, int kind, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,206 @@
+// C entry points over the UNMODIFIED reference WENO sources (src_WENO/fluid.cpp
+// and src_WENO/solver.cpp, compiled from where they lie with the Eigen/MPI
+// shims in oracle/shim).  Test infrastructure: this library is the checker the
+// GPU path is compared against, never part of the product.
+//
+// Array convention at this boundary (the same as the GPU library's C ABI):
+//   U      double[4][ny][nx]  conserved fields rho, rho*u, rho*v, E; row i = y
+//                             index (row 0 = top, as in the .dat files), col j = x
+//   bct    int32[ny][nx]      bctype codes (0 fluid, -1 copy ghost, -3 MPI ghost)
+// The Mesh stores column-major (src_WENO/fluid.cpp:391-393); conversion happens here.
+
+#define main zk_reference_weno_main
+#include "solver.cpp"
+#undef main
+
+#include <cstdint>
+#include <thread>
+
+namespace {
+
+Mesh make_mesh(int ny, int nx, double da, double gamma, const double* U, const int* bct) {
+    Mesh m(ny, nx, da, gamma);
+    const size_t plane = static_cast<size_t>(ny) * nx;
+    for (int i = 0; i < ny; ++i)
+        for (int j = 0; j < nx; ++j) {
+            const size_t k = static_cast<size_t>(i) * nx + j;
+            m.U0(i, j) = U[0 * plane + k];
+            m.U1(i, j) = U[1 * plane + k];
+            m.U2(i, j) = U[2 * plane + k];
+            m.U3(i, j) = U[3 * plane + k];
+            m.bctype(i, j) = bct[k];
+        }
+    return m;
+}
+
+void store_U(const Mesh& m, double* U) {
+    const int ny = m.ny, nx = m.nx;
+    const size_t plane = static_cast<size_t>(ny) * nx;
+    for (int i = 0; i < ny; ++i)
+        for (int j = 0; j < nx; ++j) {
+            const size_t k = static_cast<size_t>(i) * nx + j;
+            U[0 * plane + k] = m.U0(i, j);
+            U[1 * plane + k] = m.U1(i, j);
+            U[2 * plane + k] = m.U2(i, j);
+            U[3 * plane + k] = m.U3(i, j);
+        }
+}
+
+void store_field(const MatrixXd& f, double* out) {
+    for (int i = 0; i < f.rows(); ++i)
+        for (int j = 0; j < f.cols(); ++j) out[static_cast<size_t>(i) * f.cols() + j] = f(i, j);
+}
+
+// Periodic image of the 3-wide ring: the reference has no periodic boundary,
+// so the harness marks the ring -3 (which its own ghost fill never touches)
+// and refills it before every computeRHS call.
+void fill_periodic(Mesh& m) {
+    const int ny = m.ny, nx = m.nx, iy = ny - 6, ix = nx - 6;
+    auto wrap = [](int k, int n) { return 3 + (((k - 3) % n) + n) % n; };
+    for (int i = 0; i < ny; ++i)
+        for (int j = 0; j < nx; ++j) {
+            if (m.bctype(i, j) != -3) continue;
+            const int si = wrap(i, iy), sj = wrap(j, ix);
+            m.U0(i, j) = m.U0(si, sj); m.U1(i, j) = m.U1(si, sj);
+            m.U2(i, j) = m.U2(si, sj); m.U3(i, j) = m.U3(si, sj);
+        }
+}
+
+// updateMesh (src_WENO/fluid.cpp:468-493) with a periodic refill before each
+// computeRHS; at one rank exchangeConservativeColumns is a no-op.
+void update_mesh_periodic(Mesh& mesh, double dt) {
+    const MatrixXd U0n = mesh.U0, U1n = mesh.U1, U2n = mesh.U2, U3n = mesh.U3;
+    MatrixXd dU0, dU1, dU2, dU3;
+    fill_periodic(mesh);
+    computeRHS(mesh, dt, dU0, dU1, dU2, dU3);
+    mesh.U0 = U0n + dU0; mesh.U1 = U1n + dU1; mesh.U2 = U2n + dU2; mesh.U3 = U3n + dU3;
+    fill_periodic(mesh);
+    computeRHS(mesh, dt, dU0, dU1, dU2, dU3);
+    mesh.U0 = 0.75 * U0n + 0.25 * (mesh.U0 + dU0);
+    mesh.U1 = 0.75 * U1n + 0.25 * (mesh.U1 + dU1);
+    mesh.U2 = 0.75 * U2n + 0.25 * (mesh.U2 + dU2);
+    mesh.U3 = 0.75 * U3n + 0.25 * (mesh.U3 + dU3);
+    fill_periodic(mesh);
+    computeRHS(mesh, dt, dU0, dU1, dU2, dU3);
+    mesh.U0 = (1.0 / 3.0) * U0n + (2.0 / 3.0) * (mesh.U0 + dU0);
+    mesh.U1 = (1.0 / 3.0) * U1n + (2.0 / 3.0) * (mesh.U1 + dU1);
+    mesh.U2 = (1.0 / 3.0) * U2n + (2.0 / 3.0) * (mesh.U2 + dU2);
+    mesh.U3 = (1.0 / 3.0) * U3n + (2.0 / 3.0) * (mesh.U3 + dU3);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Timing emulation of the reference's MPI run with `nthreads` ranks: the grid
+// is split into x-slabs by the reference's own splitMeshVertically
+// (fluid.cpp), and each slab runs nsteps x updateMesh on its own thread.  With
+// the single-rank MPI stub the 3-column halo exchange between slabs is a no-op
+// (a memcpy of 3 columns in the real build), so the numbers are a throughput
+// sample only.  Returns the wall time in ms of the slowest slab; *cells gets
+// the number of cells the slabs update.
+double refw_step_slabs_timed(int ny, int nx, double da, double gamma, const double* state,
+                               const int* bct, double dt, int nsteps, int nthreads, long* cells) {
+    Mesh full = make_mesh(ny, nx, da, gamma, state, bct);
+    vector<Mesh> subs = splitMeshVertically(full, nthreads);
+    long n = 0;
+    for (auto& m : subs)
+        for (int i = 3; i < m.ny - 3; ++i)
+            for (int j = 3; j < m.nx - 3; ++j) n += (m.bctype(i, j) == 0);
+    *cells = n;
+    std::vector<double> ms(subs.size(), 0.0);
+    std::vector<std::thread> th;
+    for (size_t r = 0; r < subs.size(); ++r)
+        th.emplace_back([&, r] {
+            auto t0 = now();
+            for (int s = 0; s < nsteps; ++s) updateMesh(subs[r], dt, 0, 1);
+            ms[r] = elapsed_ms(t0, now());
+        });
+    for (auto& t : th) t.join();
+    return *std::max_element(ms.begin(), ms.end());
+}
+
+// Dimensions and parameters of a case directory (params.txt: nx ny da gamma).
+int refw_case_info(const char* dir, int* ny, int* nx, double* da, double* gamma) {
+    try {
+        Mesh m{std::string(dir)};
+        *ny = m.ny; *nx = m.nx; *da = m.da; *gamma = m.gamma;
+        return 0;
+    } catch (...) { return 1; }
+}
+
+// Mesh(folder) (src_WENO/fluid.cpp:68-94): primitive -> conserved, plus bctype.
+int refw_load_case(const char* dir, double* U, int* bct) {
+    try {
+        Mesh m{std::string(dir)};
+        store_U(m, U);
+        for (int i = 0; i < m.ny; ++i)
+            for (int j = 0; j < m.nx; ++j) bct[static_cast<size_t>(i) * m.nx + j] = m.bctype(i, j);
+        return 0;
+    } catch (...) { return 1; }
+}
+
+// computeRHS (src_WENO/fluid.cpp:328-463).  U is updated in place with the
+// ghost fill, exactly as the reference mutates the Mesh; dU includes dt.
+int refw_rhs(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
+             double* dU) {
+    Mesh m = make_mesh(ny, nx, da, gamma, U, bct);
+    MatrixXd d0, d1, d2, d3;
+    computeRHS(m, dt, d0, d1, d2, d3);
+    store_U(m, U);
+    const size_t plane = static_cast<size_t>(ny) * nx;
+    store_field(d0, dU + 0 * plane); store_field(d1, dU + 1 * plane);
+    store_field(d2, dU + 2 * plane); store_field(d3, dU + 3 * plane);
+    return 0;
+}
+
+// nsteps x updateMesh (src_WENO/fluid.cpp:468-493) at one rank.
+int refw_step(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
+              int nsteps, int periodic) {
+    Mesh m = make_mesh(ny, nx, da, gamma, U, bct);
+    for (int s = 0; s < nsteps; ++s) {
+        if (periodic) update_mesh_periodic(m, dt);
+        else updateMesh(m, dt, 0, 1);
+    }
+    store_U(m, U);
+    return 0;
+}
+
+// Same as refw_step, returning the wall time spent inside updateMesh only
+// (the reference's own timer placement, src_WENO/solver.cpp:174-176).
+double refw_step_timed(int ny, int nx, double da, double gamma, double* U, const int* bct,
+                       double dt, int nsteps) {
+    Mesh m = make_mesh(ny, nx, da, gamma, U, bct);
+    double ms = 0.0;
+    for (int s = 0; s < nsteps; ++s) {
+        auto t0 = now();
+        updateMesh(m, dt, 0, 1);
+        ms += elapsed_ms(t0, now());
+    }
+    store_U(m, U);
+    return ms;
+}
+
+// computeMaxSpeed (src_WENO/fluid.cpp:539-553): all cells, ghosts included.
+double refw_max_speed(int ny, int nx, double da, double gamma, const double* U, const int* bct) {
+    Mesh m = make_mesh(ny, nx, da, gamma, U, bct);
+    return computeMaxSpeed(m, gamma);
+}
+
+// recoverPrimitives (src_WENO/fluid.cpp:500-515): prim = [rho, u, v, p] planes.
+int refw_recover(int ny, int nx, double da, double gamma, const double* U, const int* bct,
+                 double* prim) {
+    Mesh m = make_mesh(ny, nx, da, gamma, U, bct);
+    recoverPrimitives(m);
+    const size_t plane = static_cast<size_t>(ny) * nx;
+    store_field(m.rho, prim + 0 * plane); store_field(m.u, prim + 1 * plane);
+    store_field(m.v, prim + 2 * plane); store_field(m.p, prim + 3 * plane);
+    return 0;
+}
+
+// hllcFlux (src_WENO/fluid.cpp:268-317), x direction.
+void refw_hllc(const double* UL, const double* UR, double gamma, double* F) {
+    hllcFlux(UL[0], UL[1], UL[2], UL[3], UR[0], UR[1], UR[2], UR[3], gamma, F[0], F[1], F[2], F[3]);
+}
+
+}  // extern "C"

@@ -1,0 +1,190 @@
+"""GPU WENO5 FP64 path against the reference (through the C ABI).
+
+The FP64 path reproduces the reference's arithmetic op for op (nvcc
+--fmad=false), so against the strict reference build (-ffp-contract=off) the
+bar is BIT-EXACT equality; against the Makefile-faithful build (FMA
+contraction) it is 1e-10 relative L-inf per conserved field.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import rel_linf
+
+pytestmark = pytest.mark.gpu
+
+WENO = ["weno_fq_24x24_s3", "weno_fq_23x37_s11", "weno_fq_7x7_s5", "weno_obstacle_26",
+        "weno_jet_40x20", "weno_allghost_12"]
+
+
+def solver(b, da, gamma, **kw):
+    from zuikakucfd_b200 import Solver
+    s = Solver(method="weno", **kw)
+    s.set_mesh(b.shape[0], b.shape[1], da, gamma, b)
+    return s
+
+
+@pytest.mark.parametrize("name", WENO)
+def test_steps_bit_exact(golden, golden_meta, name):
+    m = golden_meta[name]
+    U0, b = golden[f"{name}/U0"], golden[f"{name}/bct"]
+    with solver(b, m["da"], m["gamma"]) as s:
+        s.set_state(U0)
+        s.step(m["dt"], 1)
+        assert np.array_equal(s.get_state(), golden[f"{name}/strict_1"])
+        s.step(m["dt"], 9)
+        out = s.get_state()
+        assert np.array_equal(out, golden[f"{name}/strict_10"])
+        assert rel_linf(out, golden[f"{name}/faithful_10"]) < 1e-10
+        assert s.max_speed() == m["max_speed_10"]
+        assert np.array_equal(s.recover_primitives(), golden[f"{name}/prim_10"], equal_nan=True)
+
+
+@pytest.mark.parametrize("name", WENO)
+def test_rhs_fills_ghosts_in_place(golden, golden_meta, name):
+    m = golden_meta[name]
+    U0, b = golden[f"{name}/U0"], golden[f"{name}/bct"]
+    with solver(b, m["da"], m["gamma"]) as s:
+        s.set_state(U0)
+        assert s.max_speed() == m["max_speed"]
+        dU = s.rhs(m["dt"])
+        assert np.array_equal(dU, golden[f"{name}/rhs_dU"])
+        assert np.array_equal(s.get_state(), golden[f"{name}/rhs_U"])
+
+
+def test_periodic_wave(golden, golden_meta):
+    m = golden_meta["weno_wave_16"]
+    with solver(golden["weno_wave_16/bct"], m["da"], m["gamma"], boundary="periodic") as s:
+        s.set_state(golden["weno_wave_16/U0"])
+        s.step(m["dt"], 5)
+        assert np.array_equal(s.get_state(), golden["weno_wave_16/strict_5"])
+
+
+def test_reference_riemann_case_sha256(golden, golden_meta):
+    m = golden_meta["riemann256"]
+    with solver(golden["riemann256/bct"], m["da"], m["gamma"]) as s:
+        s.set_state(golden["riemann256/U0"])
+        assert s.max_speed() == m["max_speed"]
+        s.step(m["dt"], m["steps"])
+        out = s.get_state()
+    assert hashlib.sha256(out.tobytes()).hexdigest() == m["strict_sha256"]
+    assert rel_linf(out[:, ::17], golden["riemann256/faithful_20_rows"]) < 1e-10
+
+
+def test_seeded_128_sha256(golden_meta):
+    from zuikakucfd_b200 import cases
+    m = golden_meta["weno_fq128_s42"]
+    c = cases.four_quadrant(128, seed=42)
+    with solver(c.bctype, c.da, c.gamma) as s:
+        s.set_state(c.conserved())
+        s.step(m["dt"], m["steps"])
+        out = s.get_state()
+    assert hashlib.sha256(out.tobytes()).hexdigest() == m["strict_sha256"]
+
+
+def test_config0_size_against_oracle(restatement):
+    """The WENO config's own size (256^2 four-quadrant, CFL 0.5), 40 steps,
+    bit-exact against the CPU oracle."""
+    from zuikakucfd_b200 import cases
+    c = cases.four_quadrant(256, seed=0)
+    dt = cases.cfl_dt(c, 0.5)
+    ref = restatement.weno_step(c.conserved(), c.bctype, c.da, c.gamma, dt, 40)
+    with solver(c.bctype, c.da, c.gamma) as s:
+        s.set_state(c.conserved())
+        s.step(dt, 40)
+        assert np.array_equal(s.get_state(), ref)
+
+
+def test_periodic_mass_conservation_1024():
+    """1024^2 periodic wave: the flux form telescopes (each interface flux is
+    computed once, from the same six cells on both sides of the seam), so the
+    interior mass changes only by summation rounding."""
+    from zuikakucfd_b200 import cases
+    w = cases.smooth_wave(1018)
+    U0 = w.conserved()
+    dt = 0.4 * w.da / 2.5
+    with solver(w.bctype, w.da, w.gamma, boundary="periodic") as s:
+        s.set_state(U0)
+        s.step(dt, 5)
+        out = s.get_state()
+    m0 = U0[0, 3:-3, 3:-3].sum()
+    m1 = out[0, 3:-3, 3:-3].sum()
+    assert abs(m1 - m0) / m0 < 1e-12
+    assert not np.array_equal(out, U0)
+
+
+def test_jet_full_size_determinism():
+    """The jet config's grid (2048x1024, Mach ~80 inflow): two runs bitwise
+    equal (race check) and the state stays finite and positive."""
+    from zuikakucfd_b200 import cases
+    j = cases.high_mach_jet(2048, 1024)
+    dt = 0.4 * j.da / (30.0 + np.sqrt(j.gamma * 0.4127 / 5.0))
+    outs = []
+    for _ in range(2):
+        with solver(j.bctype, j.da, j.gamma) as s:
+            s.set_state(j.conserved())
+            s.step(dt, 20)
+            outs.append(s.get_state())
+            assert s.status_word() == 0
+    assert np.array_equal(outs[0], outs[1])
+    assert np.isfinite(outs[0]).all() and outs[0][0].min() > 0
+
+
+def test_load_case_matches_host_reader(tmp_path):
+    from zuikakucfd_b200 import Solver, cases
+    from zuikakucfd_b200.fluid import read_case, primitive_to_conserved
+    c = cases.four_quadrant(40, seed=8, ny=33)
+    cases.write_case(c, tmp_path)
+    with Solver(method="weno") as s:
+        s.load_case(tmp_path)
+        r = read_case(tmp_path)
+        assert np.array_equal(s.get_state(), primitive_to_conserved(r["rho"], r["u"], r["v"], r["p"], r["gamma"]))
+
+
+def test_status_word_flags_bad_states():
+    from zuikakucfd_b200 import cases
+    c = cases.four_quadrant(32, seed=1)
+    U = c.conserved()
+    U[0, 10, 10] = np.nan
+    with solver(c.bctype, c.da, c.gamma) as s:
+        s.set_state(U)
+        s.step(1e-4, 1)
+        assert s.status_word() & 1
+        U = c.conserved()
+        s.set_state(U)
+        s.step(1e-4, 1)
+        assert s.status_word() == 0
+
+
+def test_errors_are_reported_not_thrown():
+    from zuikakucfd_b200 import Solver
+    from zuikakucfd_b200._native import ZkError
+    with Solver(method="weno") as s:
+        with pytest.raises(ZkError, match="ZK_ERR_STATE"):
+            s.step(1e-3, 1)
+        b = np.zeros((16, 16), np.int32)
+        with pytest.raises(ZkError, match="ZK_ERR_ARG"):
+            s.set_mesh(16, 16, 0.1, 0.9, b)       # gamma <= 1
+        s.set_mesh(16, 16, 0.1, 1.4, b)
+        with pytest.raises(ZkError, match="ZK_ERR_ARG"):
+            s.step(-1.0, 1)
+        with pytest.raises(ZkError, match="ZK_ERR_UNSUPPORTED"):
+            s.limit()
+
+
+def test_reference_shaped_api(tmp_path):
+    from zuikakucfd_b200 import Mesh, cases, computeMaxSpeed, computeRHS, recoverPrimitives, updateMesh
+    c = cases.four_quadrant(24, seed=3)
+    cases.write_case(c, tmp_path)
+    mesh = Mesh(tmp_path)
+    lam = computeMaxSpeed(mesh, mesh.gamma)
+    dt = 0.5 * mesh.da / lam
+    U0 = mesh.state.copy()
+    dU = computeRHS(mesh, dt)
+    assert dU.shape == (4, 24, 24)
+    updateMesh(mesh, dt, 0, 1)
+    recoverPrimitives(mesh)
+    assert mesh.rho.shape == (24, 24) and np.isfinite(mesh.p).all()
+    assert not np.array_equal(mesh.U0, U0[0])
+    mesh.close()

@@ -1,0 +1,156 @@
+"""Seeded initial conditions in the reference's case format.
+
+Conventions follow the reference's generator notebook (gen.ipynb, cells 0-1):
+``da = L / nx``; row 0 is the TOP of the domain (``yc = y_max - (i + 0.5) da``)
+and column 0 the left (``xc = x_min + (j + 0.5) da``); the boundary ring lies
+inside the ``ny x nx`` grid; files are ``params.txt`` ("nx ny da gamma") plus
+row-major text matrices ``rho/u/v/p/bctype.dat``.
+
+Randomised states use ``numpy.random.default_rng(seed)``, drawing the four
+quadrants in the fixed order NE, NW, SW, SE and (rho, u, v, p) within each.
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+
+@dataclass
+class Case:
+    name: str
+    ny: int
+    nx: int
+    da: float
+    gamma: float
+    rho: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    p: np.ndarray
+    bctype: np.ndarray
+    periodic: bool = False
+    seed: int | None = None
+
+    def conserved(self) -> np.ndarray:
+        """U[4][ny][nx] = rho, rho u, rho v, E (src_WENO/fluid.cpp:86-93)."""
+        r, u, v, p, g = self.rho, self.u, self.v, self.p, self.gamma
+        return np.stack([r, r * u, r * v, p / (g - 1.0) + 0.5 * r * (u * u + v * v)])
+
+    def dg_state(self, order: int) -> np.ndarray:
+        """dof[4][NM][ny][nx] with mode 0 = the cell values (initDGModes,
+        src_DG/fluid.cpp:173-182)."""
+        nm = (order + 1) ** 2
+        d = np.zeros((4, nm, self.ny, self.nx))
+        d[:, 0] = self.conserved()
+        return d
+
+    @property
+    def fluid_cells(self) -> int:
+        """Cells the RHS updates: bctype 0 inside [3, ny-3) x [3, nx-3)."""
+        return int((self.bctype[3:-3, 3:-3] == 0).sum())
+
+
+def _ring(ny: int, nx: int, width: int = 3, code: int = -1) -> np.ndarray:
+    b = np.zeros((ny, nx), np.int32)
+    b[:width, :] = code
+    b[-width:, :] = code
+    b[:, :width] = code
+    b[:, -width:] = code
+    return b
+
+
+def four_quadrant(n: int = 256, seed: int = 0, gamma: float = 1.4, ny: int | None = None,
+                  split: float = 0.5, ring_code: int = -1) -> Case:
+    """Four constant quadrants on [0,1] x [0, ny/n], split at (split, split) by
+    cell centre; each quadrant rho,p ~ U[0.1,2], u,v ~ U[-1,1]; 3-cell ring."""
+    nx = int(n)
+    ny = int(ny or n)
+    da = 1.0 / nx
+    rng = np.random.default_rng(seed)
+    # NE, NW, SW, SE; (rho, u, v, p) each
+    q = []
+    for _ in range(4):
+        rho = rng.uniform(0.1, 2.0)
+        u = rng.uniform(-1.0, 1.0)
+        v = rng.uniform(-1.0, 1.0)
+        p = rng.uniform(0.1, 2.0)
+        q.append((rho, u, v, p))
+    xc = (np.arange(nx) + 0.5) * da
+    yc = ny * da - (np.arange(ny) + 0.5) * da
+    X, Y = np.meshgrid(xc, yc)
+    east, north = X >= split, Y >= split
+    idx = np.where(north & east, 0, np.where(north, 1, np.where(east, 3, 2)))
+    tab = np.array(q)
+    f = tab[idx]
+    return Case(f"four_quadrant_{nx}x{ny}_s{seed}", ny, nx, da, gamma, f[..., 0], f[..., 1],
+                f[..., 2], f[..., 3], _ring(ny, nx, 3, ring_code), seed=seed)
+
+
+def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0.2,
+                length: float = 2.0) -> Case:
+    """rho = 1 + a sin(pi (x + y)), u = v = 1, p = 1 on [0, length]^2, periodic:
+    n_interior^2 fluid cells plus a 3-cell ring marked -3 holding the periodic
+    images.  Exact solution at time t: the initial field shifted by (t, t)."""
+    n = int(n_interior)
+    h = length / n
+    N = n + 6
+    k = np.arange(N)
+    xc = ((k - 3) % n + 0.5) * h             # periodic image coordinate
+    yc = length - ((k - 3) % n + 0.5) * h
+    X, Y = np.meshgrid(xc, yc)
+    rho = 1.0 + amplitude * np.sin(np.pi * (X + Y))
+    one = np.ones((N, N))
+    return Case(f"smooth_wave_{n}", N, N, h, gamma, rho, one.copy(), one.copy(), one.copy(),
+                _ring(N, N, 3, -3), periodic=True)
+
+
+def smooth_wave_exact(case: Case, t: float, amplitude: float = 0.2, length: float = 2.0) -> np.ndarray:
+    """Cell-centre density of the translated wave at time t (interior cells)."""
+    n = case.nx - 6
+    h = length / n
+    c = (np.arange(n) + 0.5) * h
+    X, Y = np.meshgrid(c, length - c)
+    return 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y - t)))
+
+
+def high_mach_jet(nx: int = 2048, ny: int = 1024, gamma: float = 5.0 / 3.0, u_jet: float = 30.0,
+                  rho_jet: float = 5.0, rho_amb: float = 0.5, p_amb: float = 0.4127,
+                  half_width: float = 0.05) -> Case:
+    """Jet on [0,1] x [-0.25,0.25] (da = 1/nx).  Following the HighMachJet
+    case: columns 0-2 of the rows inside the ring are bctype-0 cells that the
+    RHS loop never updates (frozen inflow); the band |yc| < half_width carries
+    (rho_jet, u_jet); -1 ring elsewhere."""
+    da = 1.0 / nx
+    y_top = ny * da / 2.0
+    yc = y_top - (np.arange(ny) + 0.5) * da
+    rho = np.full((ny, nx), rho_amb)
+    u = np.zeros((ny, nx))
+    v = np.zeros((ny, nx))
+    p = np.full((ny, nx), p_amb)
+    band = np.abs(yc) < half_width
+    rho[band, :3] = rho_jet
+    u[band, :3] = u_jet
+    b = _ring(ny, nx, 3, -1)
+    b[3:-3, :3] = 0
+    return Case(f"high_mach_jet_{nx}x{ny}", ny, nx, da, gamma, rho, u, v, p, b)
+
+
+def write_case(case: Case, folder: str | os.PathLike, fmt: str = "%.17e") -> Path:
+    """Write params.txt + rho/u/v/p/bctype.dat in the reference's format."""
+    d = Path(folder)
+    d.mkdir(parents=True, exist_ok=True)
+    (d / "params.txt").write_text(f"{case.nx} {case.ny} {case.da:.17e} {case.gamma!r}\n")
+    for name in ("rho", "u", "v", "p"):
+        np.savetxt(d / f"{name}.dat", getattr(case, name), fmt=fmt, delimiter=" ")
+    np.savetxt(d / "bctype.dat", case.bctype, fmt="%d", delimiter=" ")
+    return d
+
+
+def cfl_dt(case: Case, cfl: float = 0.5) -> float:
+    """dt = cfl * da / lambda0, lambda0 = max over ALL cells of |u| + a (the
+    reference's computeMaxSpeed rule, src_WENO/fluid.cpp:539-553)."""
+    a = np.sqrt(case.gamma * case.p / case.rho)
+    lam = float(np.max(np.sqrt(case.u ** 2 + case.v ** 2) + a))
+    return cfl * case.da / lam

@@ -1,0 +1,49 @@
+// Internal definition of the opaque zk_ctx and the hooks between the API
+// layer (zk_api.cu) and the method-specific drivers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "zk_common.cuh"
+#include "zuikaku.h"
+
+struct zk_ctx {
+    zk_options opt{};
+    zk::Grid g{};
+    double da = 0.0, gamma = 0.0;
+    int nm = 1;    // modes per variable (1 for WENO)
+    int nvar = 4;  // planes of the state (4 * nm)
+    int sms = 148;
+    std::vector<int32_t> bct;  // host copy of bctype, row-major ny x nx
+
+    double* Un = nullptr;  // FP64 state (the step's U^n, updated in place by the last stage)
+    double* S1 = nullptr;  // stage scratch
+    double* S2 = nullptr;  // stage scratch
+    double* d_tmp = nullptr;
+    float* F1 = nullptr;  // FP32 stage states of the mixed-precision path
+    float* F2 = nullptr;
+    int8_t* kind = nullptr;   // per-cell kind byte (zk::KIND_*), pitched
+    int32_t* gsrc = nullptr;  // fill source (pitched linear index) of ghost cells
+    unsigned long long* d_max = nullptr;
+    uint32_t* d_status = nullptr;
+    double* d_phic = nullptr;  // DG basis at the 4 cell corners, [NM][4]
+
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void* dg = nullptr;  // DG driver state
+};
+
+int zk_internal_fail(int code, const char* msg);
+
+// DG driver (dg_driver.cu)
+int zk_dg_setup(zk_ctx* c);
+void zk_dg_release(zk_ctx* c);
+int zk_dg_step(zk_ctx* c, double dt);
+int zk_dg_rhs(zk_ctx* c, double* dU_dev);
+int zk_dg_limit(zk_ctx* c);
+
+// WENO mixed-precision driver (weno_mixed.cu)
+int zk_weno_mixed_setup(zk_ctx* c);
+int zk_weno_mixed_step(zk_ctx* c, double dt);

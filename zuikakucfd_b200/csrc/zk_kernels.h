@@ -1,0 +1,26 @@
+// Host-side launchers of the sm_100a kernels (one per .cu file group).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "zk_common.cuh"
+
+namespace zk {
+
+// ---- FP64 reference-arithmetic kernels (built with --fmad=false) ----------
+cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
+                                   const int8_t* kind, const int32_t* gsrc, const Grid& g,
+                                   double dtdx, double dtdy, double gamma, int stage,
+                                   uint32_t* status, cudaStream_t s);
+
+cudaError_t launch_fill_ghosts(double* U, const int8_t* kind, const int32_t* gsrc, const Grid& g,
+                               int nvar, int nm, int sms, cudaStream_t s);
+cudaError_t launch_max_speed_weno(const double* U, const Grid& g, double gamma,
+                                  unsigned long long* out, int sms, cudaStream_t s);
+cudaError_t launch_max_speed_dg(const double* dof, const int8_t* kind, const Grid& g, int nm,
+                                double gamma, const double* phic, unsigned long long* out, int sms,
+                                cudaStream_t s);
+cudaError_t launch_recover(const double* U, const Grid& g, int nm, double gamma, double* prim,
+                           int sms, cudaStream_t s);
+
+}  // namespace zk
