@@ -51,64 +51,60 @@ def make_workload(name: str, rank: int):
                     desc="high-Mach jet 2048x1024 (rho=5,u=30 band, gamma=5/3), WENO5+HLLC+SSP-RK3")
     if name == "weno_fq_2048":
         c = cases.four_quadrant(2048, seed=seed)
-        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.5),
-                    desc="seeded four-quadrant Riemann 2048x2048, WENO5+HLLC+SSP-RK3, CFL 0.5")
+        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.4),
+                    desc=f"seeded four-quadrant Riemann 2048x2048 (seed {seed}), WENO5+HLLC+SSP-RK3, CFL 0.4")
     raise SystemExit(f"unknown workload {name}")
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled during the timed region: NVML
+    polled every ~2 ms from a thread (the timed call releases the GIL)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, device: int):
         self.device = device
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+            idx = int(vis.split(",")[self.device]) if vis else self.device
+            self.h = nv.nvmlDeviceGetHandleByIndex(idx)
+            self.nv = nv
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
-        except OSError:
-            self.proc = None
+        except Exception:
+            self.nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((float(mhz), int(r)))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        self._stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=2)
 
     def summary(self) -> dict:
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = max(smax, float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [m for m, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items() if r & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(sm), "source": "NVML, polled every 2 ms"}
 
 
 def dist_setup(n_gpus: int):
@@ -200,14 +196,43 @@ def run_reference_arm(args, w) -> dict:
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_e2e(s, w, U0, args, world, dofs, pg) -> dict:
+    """End to end through the public C ABI with host buffers: the reference
+    driver's loop (computeMaxSpeed -> dt on the host -> updateMesh,
+    src_WENO/solver.cpp:159-178), the state uploaded from pinned host memory at
+    the start and read back at the end, all inside the timed region."""
+    import ctypes as C
+    import torch
+    from zuikakucfd_b200 import _native as N
+    host_in = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    state_bytes = host_in.numel() * 8
+    L = N.lib()
+    lam = C.c_double()
+    barrier(pg)
+    t0 = time.perf_counter()
+    N.check(L.zk_set_state(s._h, C.cast(host_in.data_ptr(), C.POINTER(C.c_double))))
+    for _ in range(args.steps):
+        N.check(L.zk_max_speed(s._h, C.byref(lam)))
+        N.check(L.zk_step(s._h, C.c_double(w["dt"]), 1))
+    N.check(L.zk_get_state(s._h, C.cast(host_out.data_ptr(), C.POINTER(C.c_double))))
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0)
+    return {"value": world * dofs * args.steps / e2e_s, "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes / args.steps + 8,
+            "d2h_bytes_per_step": state_bytes / args.steps + 8,
+            "what": "reference driver loop per step: zk_max_speed (8 B read back) + zk_step(dt); "
+                    "state H2D from pinned host at start, D2H at end, amortised per step; host wall clock"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="weno_jet_2048x1024")
+    ap.add_argument("--workload", default="weno_fq_2048")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -243,27 +268,9 @@ def main():
     # end to end through the public API with host buffers: the reference
     # driver's loop (computeMaxSpeed -> dt on the host -> updateMesh), state
     # uploaded from pinned host memory at the start and read back at the end
-    import torch
-    host_in = torch.from_numpy(np.ascontiguousarray(U0)).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    state_bytes = host_in.numel() * 8
-    barrier(pg)
-    t0 = time.perf_counter()
-    import ctypes as C
-    from zuikakucfd_b200 import _native as N
-    L = N.lib()
-    N.check(L.zk_set_state(s._h, C.cast(host_in.data_ptr(), C.POINTER(C.c_double))))
-    lam = C.c_double()
-    for _ in range(args.steps):
-        N.check(L.zk_max_speed(s._h, C.byref(lam)))
-        N.check(L.zk_step(s._h, C.c_double(w["dt"]), 1))
-    N.check(L.zk_get_state(s._h, C.cast(host_out.data_ptr(), C.POINTER(C.c_double))))
-    e2e_s = allreduce_max(pg, time.perf_counter() - t0)
-    e2e = {"value": world * dofs * args.steps / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": state_bytes / args.steps + 8,
-           "d2h_bytes_per_step": state_bytes / args.steps + 8,
-           "what": "reference driver loop per step: zk_max_speed (8 B read back) + zk_step(dt); "
-                   "state H2D from pinned host at start, D2H at end, amortised per step"}
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(s, w, U0, args, world, dofs, pg)
 
     out = None
     if rank == 0:
@@ -286,7 +293,7 @@ def main():
                "config": {"workload": args.workload, "desc": w["desc"], "grid": [c.ny, c.nx],
                           "updated_cells": cells, "dof_per_cell": w["dof_per_cell"], "precision": "fp64",
                           "l2": "working set (3 FP64 states = %.0f MB) larger than the 126 MB L2" %
-                                (3 * state_bytes / 1e6),
+                                (3 * U0.nbytes / 1e6),
                           "parallelism": f"replicas x{world} (independent seeded problems)"},
                "clocks": clk.summary(), "e2e": e2e, "gpu_launches": 3 * args.steps,
                "roofline": roof, "cpu_baseline": cpu, "status_word": status, "peaks": peaks}

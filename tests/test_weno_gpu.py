@@ -85,15 +85,18 @@ def test_seeded_128_sha256(golden_meta):
 
 def test_config0_size_against_oracle(restatement):
     """The WENO config's own size (256^2 four-quadrant, CFL 0.5), 40 steps,
-    bit-exact against the CPU oracle."""
+    bit-exact against the CPU oracle.  (Seed 0 drives the reference scheme to
+    NaN within 40 steps; seed 1 runs 200 steps cleanly.)"""
     from zuikakucfd_b200 import cases
-    c = cases.four_quadrant(256, seed=0)
+    c = cases.four_quadrant(256, seed=1)
     dt = cases.cfl_dt(c, 0.5)
     ref = restatement.weno_step(c.conserved(), c.bctype, c.da, c.gamma, dt, 40)
     with solver(c.bctype, c.da, c.gamma) as s:
         s.set_state(c.conserved())
         s.step(dt, 40)
-        assert np.array_equal(s.get_state(), ref)
+        out = s.get_state()
+        assert np.isfinite(ref).all()
+        assert np.array_equal(out, ref)
 
 
 def test_periodic_mass_conservation_1024():
@@ -114,12 +117,14 @@ def test_periodic_mass_conservation_1024():
     assert not np.array_equal(out, U0)
 
 
-def test_jet_full_size_determinism():
-    """The jet config's grid (2048x1024, Mach ~80 inflow): two runs bitwise
-    equal (race check) and the state stays finite and positive."""
+def test_jet_full_size_determinism_and_nan_parity(restatement):
+    """The jet config's grid (2048x1024, Mach ~80 inflow).  The reference
+    scheme itself produces negative pressure at the jet edges at CFL >= 0.03
+    (its own HighMachJet example runs at CFL ~0.003); the GPU path must
+    reproduce that behaviour, NaNs included, and be deterministic."""
     from zuikakucfd_b200 import cases
     j = cases.high_mach_jet(2048, 1024)
-    dt = 0.4 * j.da / (30.0 + np.sqrt(j.gamma * 0.4127 / 5.0))
+    dt = 0.003 * j.da / (30.0 + np.sqrt(j.gamma * 0.4127 / 5.0))
     outs = []
     for _ in range(2):
         with solver(j.bctype, j.da, j.gamma) as s:
@@ -129,6 +134,17 @@ def test_jet_full_size_determinism():
             assert s.status_word() == 0
     assert np.array_equal(outs[0], outs[1])
     assert np.isfinite(outs[0]).all() and outs[0][0].min() > 0
+    # a small jet at CFL 0.1 goes NaN in the reference arithmetic: same bits
+    js = cases.high_mach_jet(128, 64)
+    dts = 0.1 * js.da / 30.0
+    ref = restatement.weno_step(js.conserved(), js.bctype, js.da, js.gamma, dts, 60)
+    with solver(js.bctype, js.da, js.gamma) as s:
+        s.set_state(js.conserved())
+        s.step(dts, 60)
+        out = s.get_state()
+        assert s.status_word() != 0
+    assert np.isnan(ref).any()
+    assert np.array_equal(out, ref, equal_nan=True)
 
 
 def test_load_case_matches_host_reader(tmp_path):
