@@ -38,6 +38,7 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("reduce_fp64.cu", STRICT),
     ("zk_pending.cu", []),
     ("peak.cu", []),
+    ("weno_mixed.cu", ["--use_fast_math"]),
 ]
 
 

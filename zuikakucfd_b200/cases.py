@@ -62,9 +62,14 @@ def _ring(ny: int, nx: int, width: int = 3, code: int = -1) -> np.ndarray:
 
 
 def four_quadrant(n: int = 256, seed: int = 0, gamma: float = 1.4, ny: int | None = None,
-                  split: float = 0.5, ring_code: int = -1) -> Case:
-    """Four constant quadrants on [0,1] x [0, ny/n], split at (split, split) by
-    cell centre; each quadrant rho,p ~ U[0.1,2], u,v ~ U[-1,1]; 3-cell ring."""
+                  split: float = 0.5, ring_code: int = -1, ring_outside: bool = False) -> Case:
+    """Four constant quadrants split at (split, split) by cell centre; each
+    quadrant rho,p ~ U[0.1,2], u,v ~ U[-1,1]; 3-cell ring.
+
+    Default (the notebook's convention): the n x ny grid, ring included, spans
+    [0,1] x [0, ny/n] with da = 1/n.  ring_outside=True: the n x ny cells are
+    the INTERIOR on [0,1] x [0, ny/n] (da = 1/n) and the ring lies outside it,
+    so grids of different resolution cover the same physical interior."""
     nx = int(n)
     ny = int(ny or n)
     da = 1.0 / nx
@@ -77,15 +82,21 @@ def four_quadrant(n: int = 256, seed: int = 0, gamma: float = 1.4, ny: int | Non
         v = rng.uniform(-1.0, 1.0)
         p = rng.uniform(0.1, 2.0)
         q.append((rho, u, v, p))
-    xc = (np.arange(nx) + 0.5) * da
-    yc = ny * da - (np.arange(ny) + 0.5) * da
+    if ring_outside:
+        gx, gy = nx + 6, ny + 6
+        xc = (np.arange(gx) - 3 + 0.5) * da
+        yc = ny * da - (np.arange(gy) - 3 + 0.5) * da
+    else:
+        gx, gy = nx, ny
+        xc = (np.arange(nx) + 0.5) * da
+        yc = ny * da - (np.arange(ny) + 0.5) * da
     X, Y = np.meshgrid(xc, yc)
     east, north = X >= split, Y >= split
     idx = np.where(north & east, 0, np.where(north, 1, np.where(east, 3, 2)))
     tab = np.array(q)
     f = tab[idx]
-    return Case(f"four_quadrant_{nx}x{ny}_s{seed}", ny, nx, da, gamma, f[..., 0], f[..., 1],
-                f[..., 2], f[..., 3], _ring(ny, nx, 3, ring_code), seed=seed)
+    return Case(f"four_quadrant_{gx}x{gy}_s{seed}", gy, gx, da, gamma, f[..., 0], f[..., 1],
+                f[..., 2], f[..., 3], _ring(gy, gx, 3, ring_code), seed=seed)
 
 
 def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0.2,

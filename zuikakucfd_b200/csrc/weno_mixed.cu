@@ -1,0 +1,329 @@
+// WENO5 + HLLC + SSP-RK3 stage, mixed precision (the fast path).
+//
+// Precision split:
+//   * reconstruction and HLLC fluxes in FP32 (this file is compiled with
+//     --use_fast_math: FP32 division and square root map to the MUFU
+//     approximations; FP64 arithmetic is unaffected);
+//   * faces whose 6-cell stencil touches a high-Mach cell -- E > 100 p, where
+//     recovering p = (gamma-1)(E - |m|^2 / 2 rho) from FP32 values would lose
+//     more than two of its digits to cancellation -- are evaluated in FP64;
+//   * interface fluxes are kept in FP64 in shared memory, and dU and the
+//     Shu-Osher combine are FP64: the conserved state is accumulated in FP64;
+//   * the positivity check recovers p from the FP64 result.
+//
+// Data movement: one 3D TMA tensor load (cp.async.bulk.tensor, no multicast)
+// brings the CTA's 40 x 14 x 4 FP64 box (tile + 3-cell halo, x start rounded
+// down to a 16-byte boundary) into shared memory; the completion wait is
+// bounded and reports STATUS_TIMEOUT instead of hanging.
+#include "tma.cuh"
+#include "tma_host.h"
+#include "zk_common.cuh"
+#include "zk_internal.h"
+
+namespace zk {
+namespace {
+
+constexpr int TX = 32, TY = 8, HX = TX + 6, HY = TY + 6;
+constexpr int SX = TX + 8;  // staged columns: x from j0-4 (16-byte aligned) to j0+35
+constexpr int NWARP = 9;
+constexpr int NTHREAD = NWARP * 32;
+constexpr uint8_t HIGH_MACH = 0x10;
+
+// weno5_reconstruct (src_WENO/fluid.cpp:230-263), any precision.
+template <typename T>
+__device__ __forceinline__ void weno5(T UL2, T UL1, T UP, T UR1, T UR2, T UR3, T& UL, T& UR) {
+    const T eps = T(1e-6), C1 = T(13.0 / 12.0), C2 = T(0.25);
+    const T c13 = T(1.0 / 3.0), c76 = T(7.0 / 6.0), c116 = T(11.0 / 6.0), c16 = T(1.0 / 6.0), c56 = T(5.0 / 6.0);
+    T qL0 = c13 * UL2 - c76 * UL1 + c116 * UP;
+    T qL1 = -c16 * UL1 + c56 * UP + c13 * UR1;
+    T qL2 = c13 * UP + c56 * UR1 - c16 * UR2;
+    T d0 = UL2 - T(2) * UL1 + UP, d1 = UL2 - T(4) * UL1 + T(3) * UP;
+    T d2 = UL1 - T(2) * UP + UR1, d3 = UL1 - UR1;
+    T d4 = UP - T(2) * UR1 + UR2, d5 = T(3) * UP - T(4) * UR1 + UR2;
+    T t0 = eps + (C1 * d0 * d0 + C2 * d1 * d1);
+    T t1 = eps + (C1 * d2 * d2 + C2 * d3 * d3);
+    T t2 = eps + (C1 * d4 * d4 + C2 * d5 * d5);
+    T a0 = T(0.1) / (t0 * t0), a1 = T(0.6) / (t1 * t1), a2 = T(0.3) / (t2 * t2);
+    UL = (a0 * qL0 + a1 * qL1 + a2 * qL2) / (a0 + a1 + a2);
+
+    T qR0 = c116 * UR1 - c76 * UR2 + c13 * UR3;
+    T qR1 = qL2;  // same combination of the same cells
+    T qR2 = qL1;
+    T r0 = UR1 - T(2) * UR2 + UR3, r1 = T(3) * UR1 - T(4) * UR2 + UR3;
+    T r3 = UP - UR2, r5 = UL1 - T(4) * UP + T(3) * UR1;
+    T s0 = eps + (C1 * r0 * r0 + C2 * r1 * r1);
+    T s1 = eps + (C1 * d4 * d4 + C2 * r3 * r3);  // r2 == d4
+    T s2 = eps + (C1 * d2 * d2 + C2 * r5 * r5);  // r4 == d2
+    T e0 = T(0.1) / (s0 * s0), e1 = T(0.6) / (s1 * s1), e2 = T(0.3) / (s2 * s2);
+    UR = (e0 * qR0 + e1 * qR1 + e2 * qR2) / (e0 + e1 + e2);
+}
+
+// std::min / std::max argument order of the reference, for either precision.
+template <typename T>
+__device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
+template <typename T>
+__device__ __forceinline__ T tmax(T a, T b) { return (a < b) ? b : a; }
+
+// hllcFlux (WENO variant, src_WENO/fluid.cpp:268-317), any precision.
+template <typename T>
+__device__ __forceinline__ void hllc(const T L[4], const T R[4], T gamma, T F[4]) {
+    const T eps = T(1e-12);
+    const T gm1 = gamma - T(1);
+    T rhoL = (L[0] < eps) ? eps : L[0];
+    T irL = T(1) / rhoL;
+    T uL = L[1] * irL, vL = L[2] * irL;
+    T pL = gm1 * (L[3] - T(0.5) * rhoL * (uL * uL + vL * vL));
+    pL = (pL < eps) ? eps : pL;
+    T rhoR = (R[0] < eps) ? eps : R[0];
+    T irR = T(1) / rhoR;
+    T uR = R[1] * irR, vR = R[2] * irR;
+    T pR = gm1 * (R[3] - T(0.5) * rhoR * (uR * uR + vR * vR));
+    pR = (pR < eps) ? eps : pR;
+    T aL = sqrt(gamma * pL * irL), aR = sqrt(gamma * pR * irR);
+    T sqL = sqrt(rhoL), sqR = sqrt(rhoR), iden = T(1) / (sqL + sqR);
+    T u_roe = (sqL * uL + sqR * uR) * iden;
+    T h_roe = (sqL * ((L[3] + pL) * irL) + sqR * ((R[3] + pR) * irR)) * iden;
+    T c2 = gm1 * (h_roe - T(0.5) * u_roe * u_roe);
+    T c_roe = sqrt(c2 < eps ? eps : c2);
+    T SL = tmin(uL - aL, u_roe - c_roe);
+    T SR = tmax(uR + aR, u_roe + c_roe);
+    if (SL >= T(0)) {
+        F[0] = rhoL * uL; F[1] = rhoL * uL * uL + pL; F[2] = rhoL * uL * vL; F[3] = (L[3] + pL) * uL;
+        return;
+    }
+    if (SR <= T(0)) {
+        F[0] = rhoR * uR; F[1] = rhoR * uR * uR + pR; F[2] = rhoR * uR * vR; F[3] = (R[3] + pR) * uR;
+        return;
+    }
+    T num = pR - pL + rhoL * uL * (SL - uL) - rhoR * uR * (SR - uR);
+    T den2 = rhoL * (SL - uL) - rhoR * (SR - uR);
+    if (fabs(den2) < eps) den2 = (den2 >= T(0)) ? eps : -eps;
+    T Ss = num / den2;
+    const bool left = Ss >= T(0);
+    const T rho = left ? rhoL : rhoR, u = left ? uL : uR, v = left ? vL : vR;
+    const T p = left ? pL : pR, S = left ? SL : SR, ir = left ? irL : irR;
+    const T* Us = left ? L : R;
+    T Su = S - u;
+    T c = rho * Su / (S - Ss);
+    T E = Us[3] * ir;
+    T s3 = c * (E + (Ss - u) * (Ss + p / (rho * Su)));
+    F[0] = rho * u + S * (c - Us[0]);
+    F[1] = rho * u * u + p + S * (c * Ss - Us[1]);
+    F[2] = rho * u * v + S * (c * v - Us[2]);
+    F[3] = (Us[3] + p) * u + S * (s3 - Us[3]);
+}
+
+struct MixedArgs {
+    const double* Ucur;  // stage input (ghosts unfilled); the tensor map covers it
+    const double* Un;
+    double* Uout;  // may alias Un at stage 3 (read-before-write per cell)
+    const int8_t* kind;
+    const int32_t* gsrc;
+    Grid g;
+    double dtdx, dtdy, gamma;
+    int stage;
+    uint32_t* status;
+};
+
+__global__ void __launch_bounds__(NTHREAD, 3)
+    weno_stage_mixed_kernel(const __grid_constant__ CUtensorMap tmap, MixedArgs a) {
+    __shared__ __align__(128) double stg[4][HY][SX];  // TMA destination, FP64, ghosts fixed up in place
+    __shared__ float sU[4][HY][HX];                   // FP32 copy of the tile + halo
+    __shared__ double sFx[4][TY][TX + 1];
+    __shared__ double sFy[4][TY + 1][TX];
+    __shared__ uint8_t sK[HY][HX];                    // kind | HIGH_MACH
+    __shared__ __align__(8) uint64_t bar;
+
+    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TY;
+    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
+    const size_t plane = a.g.plane;
+
+    // 1. TMA: the 40 x 14 x 4 box starting at (j0-4, i0-3, 0); out-of-range
+    //    elements arrive as zeros
+    if (threadIdx.x == 0) {
+        tma_prefetch_desc(&tmap);
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, (uint32_t)sizeof(stg));
+        tma_load_3d(&stg[0][0][0], &tmap, &bar, j0 - 4, i0 - 3, 0);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) {
+            atomicOr(a.status, STATUS_TIMEOUT);
+            mbar_wait_bounded(&bar, 0);  // give a late copy a second bounded chance to land
+        }
+        return;
+    }
+
+    // 2. ghost fill from the source map, FP32 copy, high-Mach flags
+    const double gm1 = a.gamma - 1.0;
+    for (int t = threadIdx.x; t < HY * HX; t += NTHREAD) {
+        const int r = t / HX, c = t - r * HX;
+        const int gi = i0 - 3 + r, gj = j0 - 3 + c;
+        uint8_t kd = KIND_PASSIVE;
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v[q] = stg[q][r][c + 1];
+        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+            const size_t k = (size_t)gi * pitch + gj;
+            kd = a.kind[k] & KIND_MASK;
+            if (kd >= KIND_COPY) {
+                const size_t s = (size_t)a.gsrc[k];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    v[q] = a.Ucur[q * plane + s];
+                    stg[q][r][c + 1] = v[q];
+                }
+            }
+            const double ke = 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0];
+            const double p = gm1 * (v[3] - ke);
+            if (!(p > 0.0) || v[3] > 100.0 * p) kd |= HIGH_MACH;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) sU[q][r][c] = (float)v[q];
+        sK[r][c] = kd;
+    }
+    __syncthreads();
+
+    // 3. interface fluxes, once per face (warp tasks as in the FP64 kernel)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float gf = (float)a.gamma;
+    for (int task = warp; task < 2 * TY + 2; task += NWARP) {
+        const bool xdir = task <= TY;
+        int r, c;
+        if (xdir) {
+            if (task < TY) { r = task; c = lane; }
+            else { if (lane >= TY) continue; r = lane; c = TX; }
+            if ((sK[r + 3][c + 2] & KIND_MASK) != KIND_UPDATED && (sK[r + 3][c + 3] & KIND_MASK) != KIND_UPDATED)
+                continue;
+        } else {
+            r = task - TY - 1; c = lane;
+            if ((sK[r + 2][c + 3] & KIND_MASK) != KIND_UPDATED && (sK[r + 3][c + 3] & KIND_MASK) != KIND_UPDATED)
+                continue;
+        }
+        // stencil cell n (0..5) at smem (rr, cc)
+        auto R_ = [&](int n) { return xdir ? r + 3 : r + n; };
+        auto C_ = [&](int n) { return xdir ? c + n : c + 3; };
+        uint8_t hm = 0;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) hm |= sK[R_(n)][C_(n)];
+        double F[4];
+        if (hm & HIGH_MACH) {
+            double QL[4], QR[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                weno5<double>(stg[q][R_(0)][C_(0) + 1], stg[q][R_(1)][C_(1) + 1], stg[q][R_(2)][C_(2) + 1],
+                              stg[q][R_(3)][C_(3) + 1], stg[q][R_(4)][C_(4) + 1], stg[q][R_(5)][C_(5) + 1],
+                              QL[q], QR[q]);
+            if (!xdir) {
+                double t = QL[1]; QL[1] = QL[2]; QL[2] = t;
+                t = QR[1]; QR[1] = QR[2]; QR[2] = t;
+            }
+            hllc<double>(QL, QR, a.gamma, F);
+        } else {
+            float QL[4], QR[4], Ff[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                weno5<float>(sU[q][R_(0)][C_(0)], sU[q][R_(1)][C_(1)], sU[q][R_(2)][C_(2)], sU[q][R_(3)][C_(3)],
+                             sU[q][R_(4)][C_(4)], sU[q][R_(5)][C_(5)], QL[q], QR[q]);
+            if (!xdir) {
+                float t = QL[1]; QL[1] = QL[2]; QL[2] = t;
+                t = QR[1]; QR[1] = QR[2]; QR[2] = t;
+            }
+            hllc<float>(QL, QR, gf, Ff);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) F[q] = (double)Ff[q];
+        }
+        if (xdir) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sFx[q][r][c] = F[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sFy[q][r][c] = F[q];
+        }
+    }
+    __syncthreads();
+
+    // 4. dU (FP64) and the Shu-Osher combine (FP64) for every cell of the tile
+    uint32_t flags = 0;
+    for (int t = threadIdx.x; t < TY * TX; t += NTHREAD) {
+        const int r = t / TX, c = t - r * TX;
+        const int gi = i0 + r, gj = j0 + c;
+        if (gi >= ny || gj >= nx) continue;
+        const size_t k = (size_t)gi * pitch + gj;
+        const bool upd = (sK[r + 3][c + 3] & KIND_MASK) == KIND_UPDATED;
+        double d[4] = {0.0, 0.0, 0.0, 0.0};
+        if (upd) {
+            // y fluxes carry the normal momentum in slot 1 (src_WENO/fluid.cpp:457-460)
+            d[0] = -(a.dtdx * (sFx[0][r][c + 1] - sFx[0][r][c]) + a.dtdy * (sFy[0][r + 1][c] - sFy[0][r][c]));
+            d[1] = -(a.dtdx * (sFx[1][r][c + 1] - sFx[1][r][c]) + a.dtdy * (sFy[2][r + 1][c] - sFy[2][r][c]));
+            d[2] = -(a.dtdx * (sFx[2][r][c + 1] - sFx[2][r][c]) + a.dtdy * (sFy[1][r + 1][c] - sFy[1][r][c]));
+            d[3] = -(a.dtdx * (sFx[3][r][c + 1] - sFx[3][r][c]) + a.dtdy * (sFy[3][r + 1][c] - sFy[3][r][c]));
+        }
+        double o[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double un = a.Un[q * plane + k];
+            const double v = stg[q][r + 3][c + 4];
+            if (a.stage == 1) o[q] = un + d[q];
+            else if (a.stage == 2) o[q] = 0.75 * un + 0.25 * (v + d[q]);
+            else o[q] = (1.0 / 3.0) * un + (2.0 / 3.0) * (v + d[q]);
+        }
+        if (upd) {
+            if (isnan(o[0]) || isnan(o[1]) || isnan(o[2]) || isnan(o[3])) flags |= STATUS_NAN;
+            if (!(o[0] > 0.0)) flags |= STATUS_RHO;
+            else if (!(gm1 * (o[3] - 0.5 * (o[1] * o[1] + o[2] * o[2]) / o[0]) > 0.0)) flags |= STATUS_P;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a.Uout[q * plane + k] = o[q];
+    }
+    flags = __reduce_or_sync(0xffffffffu, flags);
+    if (flags && lane == 0) atomicOr(a.status, flags);
+}
+
+}  // namespace
+
+cudaError_t launch_weno_stage_mixed(const CUtensorMap& tmap, const double* Ucur, const double* Un, double* Uout,
+                                    const int8_t* kind, const int32_t* gsrc, const Grid& g, double dtdx,
+                                    double dtdy, double gamma, int stage, uint32_t* status, cudaStream_t s) {
+    MixedArgs a{Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status};
+    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY);
+    weno_stage_mixed_kernel<<<grid, NTHREAD, 0, s>>>(tmap, a);
+    return cudaGetLastError();
+}
+
+// Tensor map over one FP64 WENO state: dims (x = nx, y = ny, field = 4),
+// strides pitch*8 and plane*8 bytes, box 40 x 14 x 4.
+bool encode_weno_state_map(CUtensorMap* m, const double* base, const Grid& g, const char** err) {
+    const uint64_t dims[3] = {(uint64_t)g.nx, (uint64_t)g.ny, 4};
+    const uint64_t strides[2] = {(uint64_t)g.pitch * 8, (uint64_t)g.plane * 8};
+    const uint32_t box[3] = {SX, HY, 4};
+    return encode_tmap(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, err);
+}
+
+}  // namespace zk
+
+// ---- driver: the mixed-precision WENO step ---------------------------------------
+int zk_weno_mixed_setup(zk_ctx* c) {
+    const char* err = nullptr;
+    double* bufs[3] = {c->Un, c->S1, c->S2};
+    for (int b = 0; b < 3; ++b)
+        if (!zk::encode_weno_state_map(&c->tmap[b], bufs[b], c->g, &err)) return zk_internal_fail(ZK_ERR_CUDA, err);
+    return ZK_OK;
+}
+
+int zk_weno_mixed_step(zk_ctx* c, double dt) {
+    const double dtdx = dt / c->da, dtdy = dt / c->da;
+    cudaError_t e;
+    e = zk::launch_weno_stage_mixed(c->tmap[0], c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 1,
+                                    c->d_status, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_weno_stage_mixed(c->tmap[1], c->S1, c->Un, c->S2, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma,
+                                        2, c->d_status, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_weno_stage_mixed(c->tmap[2], c->S2, c->Un, c->Un, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma,
+                                        3, c->d_status, c->stream);
+    if (e != cudaSuccess) return zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
+    return ZK_OK;
+}

@@ -2,6 +2,7 @@
 // layer (zk_api.cu) and the method-specific drivers.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <vector>
@@ -29,6 +30,8 @@ struct zk_ctx {
     unsigned long long* d_max = nullptr;
     uint32_t* d_status = nullptr;
     double* d_phic = nullptr;  // DG basis at the 4 cell corners, [NM][4]
+
+    CUtensorMap tmap[3];  // TMA maps over Un, S1, S2 (mixed WENO path)
 
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
