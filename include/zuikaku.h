@@ -136,6 +136,24 @@ int zk_state_device(zk_ctx* ctx, double** dptr, int* pitch);
  * for kernels bound by the FP pipes. */
 int zk_peak_flops(int device, int kind, double* tflops);
 
+/* No counterpart in the reference.  The FP64 WENO5 SSP-RK3 step of zk_step
+ * (same kernels, bit-identical results) for callers that cannot allocate GPU
+ * memory: applications whose device memory is owned by another allocator (a
+ * framework's caching allocator or a pool reserved at start-up) and loops
+ * that must not pay cudaMalloc's implicit synchronisation.  The caller passes
+ * device pointers to the state (planes of ny rows x pitch doubles, updated in
+ * place) and to bctype (int32 [ny][nx]); the stage states, ghost map and
+ * status word live in a fixed scratch array inside the library (about
+ * 17.3 MiB held on each GPU that loads it, until exit).  Limit:
+ * ny * pitch <= 262144 cells, else ZK_ERR_ARG.  Runs on `stream` (NULL = the
+ * default stream) of the current device.  The first call on a device looks up
+ * the scratch address and must come before any stream capture.  Calls whose
+ * GPU work overlaps race on the shared scratch.  status_out (host, may be
+ * NULL) receives the status word and makes the call synchronous. */
+int zk_weno_step_noalloc(double* state, int ny, int nx, int pitch, double da, double gamma,
+                         const int32_t* bctype, double dt, int nsteps, void* stream,
+                         uint32_t* status_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,9 @@ _SIGS = {
     "zk_step_timed": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(C.c_float)]),
     "zk_state_device": (C.c_int, [_P, C.POINTER(_D), C.POINTER(C.c_int)]),
     "zk_peak_flops": (C.c_int, [C.c_int, C.c_int, _D]),
+    "zk_weno_step_noalloc": (C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.POINTER(C.c_int32), C.c_double, C.c_int, _P,
+                                       C.POINTER(C.c_uint32)]),
 }
 
 

@@ -39,6 +39,7 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("zk_pending.cu", []),
     ("peak.cu", []),
     ("weno_mixed.cu", ["--use_fast_math"]),
+    ("noalloc.cu", []),
 ]
 
 
