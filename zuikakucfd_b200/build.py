@@ -36,7 +36,8 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("zk_api.cu", []),
     ("weno_fp64.cu", STRICT),
     ("reduce_fp64.cu", STRICT),
-    ("zk_pending.cu", []),
+    ("dg_fp64.cu", STRICT),
+    ("dg_driver.cu", []),
     ("peak.cu", []),
     ("weno_mixed.cu", ["--use_fast_math"]),
     ("noalloc.cu", []),

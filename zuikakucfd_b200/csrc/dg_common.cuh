@@ -1,0 +1,44 @@
+// Shared definitions of the DG kernels: basis tables and launch arguments.
+#pragma once
+
+#include "zk_common.cuh"
+
+namespace zk {
+
+constexpr int DG_MAXNM = 16, DG_MAXNQ = 4;
+
+// Basis values of one polynomial degree P (NQ = P+1 Gauss points, NM modes).
+struct DGTab {
+    double vw[DG_MAXNQ * DG_MAXNQ];                // volume weights w_a w_b, point p = qa*NQ+qb
+    double vphi[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];   // phi2(m, xi_a, eta_b)
+    double vdxi[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];   // d phi2 / d xi
+    double vdet[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];   // d phi2 / d eta
+    double tr[4][DG_MAXNQ][DG_MAXNM];             // traces: 0 xi=+1, 1 xi=-1, 2 eta=+1, 3 eta=-1
+    double bv[4][DG_MAXNQ][DG_MAXNM];             // trace * face weight
+    double zs[16][DG_MAXNM];                      // Zhang-Shu basis at the 4x4 Gauss points
+};
+
+// Host: tabulate P's basis (and the 4 corner values used by the CFL
+// reduction, phic[m*4+k]); upload to the calling TU's constant bank.
+void dg_make_tables(int P, DGTab* T, double* phic);
+int dg_upload_tables(int P, const DGTab& T);
+
+struct DGArgs {
+    const double* cur;   // stage input (ghosts unfilled)
+    const double* un;    // state at the start of the step
+    double* out;         // stage output (may alias un at stage 3)
+    const int8_t* kind;
+    const int32_t* gsrc;
+    double* fx;          // x-face fluxes [q][c][ny][xpitch]
+    double* fy;          // y-face fluxes [q][c][ny+1][pitch]
+    Grid g;
+    int xpitch;
+    double dt, inv2h, gamma;
+    int stage;           // 0: write d(dof)/dt only; 1..3 Shu-Osher stages
+    int limiter;         // ZK_LIMITER_*
+    int hll;             // 1: HLLE instead of HLLC
+    double s0;           // Persson threshold -4 log10 P (P<3) or -3 log10 P, from the host's libm
+    uint32_t* status;
+};
+
+}  // namespace zk
