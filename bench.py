@@ -41,18 +41,42 @@ UNIT = "DOF-updates/s"
 WENO_FLOPS_PER_CELL_STAGE = 1330.0
 
 
+# Algorithmic flops per updated cell per RK stage (face-deduplicated counts;
+# derivation in DESIGN.md).
+FLOPS_PER_CELL_STAGE = {("weno", 0): WENO_FLOPS_PER_CELL_STAGE, ("dg", 1): 1700.0, ("dg", 2): 5300.0,
+                        ("dg", 3): 13200.0}
+
+
 def make_workload(name: str, rank: int):
     from zuikakucfd_b200 import cases
     seed = 1000 + rank
     if name == "weno_jet_2048x1024":
         c = cases.high_mach_jet(2048, 1024)
-        dt = 0.4 * c.da / (30.0 + float(np.sqrt(c.gamma * 0.4127 / 5.0)))
-        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=dt,
-                    desc="high-Mach jet 2048x1024 (rho=5,u=30 band, gamma=5/3), WENO5+HLLC+SSP-RK3")
+        dt = 0.003 * c.da / (30.0 + float(np.sqrt(c.gamma * 0.4127 / 5.0)))
+        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=dt, opts={},
+                    desc="high-Mach jet 2048x1024 (rho=5,u=30 band, gamma=5/3), WENO5+HLLC+SSP-RK3, CFL 0.003")
     if name == "weno_fq_2048":
         c = cases.four_quadrant(2048, seed=seed)
-        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.4),
+        return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.4), opts={},
                     desc=f"seeded four-quadrant Riemann 2048x2048 (seed {seed}), WENO5+HLLC+SSP-RK3, CFL 0.4")
+    if name.startswith("dg") and "_fq_" in name:
+        P = int(name[2])
+        n = int(name.split("_")[-1])
+        c = cases.four_quadrant(n, seed=seed)
+        lam = c.da / cases.cfl_dt(c, 1.0)
+        dt = 0.5 * 0.9 / (2.0 * (2 * P + 1)) * c.da / lam
+        return dict(case=c, method="dg", order=P, dof_per_cell=4 * (P + 1) ** 2, dt=dt,
+                    opts={"limiter": "reference"},
+                    desc=f"seeded four-quadrant Riemann {n}x{n} (seed {seed}), DG P={P} HLLC SSP-RK3, "
+                         f"Persson+Zhang-Shu limiter, half the reference's CFL limit")
+    if name.startswith("dg") and "_wave_" in name:
+        P = int(name[2])
+        n = int(name.split("_")[-1])
+        c = cases.smooth_wave(n)
+        dt = 0.9 / (2.0 * (2 * P + 1)) * c.da / 2.74
+        return dict(case=c, method="dg", order=P, dof_per_cell=4 * (P + 1) ** 2, dt=dt,
+                    opts={"limiter": "none", "boundary": "periodic"},
+                    desc=f"periodic smooth wave {n}^2 on [0,2]^2, DG P={P} HLLC SSP-RK3, dt at the reference's CFL limit")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -148,6 +172,38 @@ def measure_peaks(device: int) -> dict:
     return out
 
 
+def _ref_state(w):
+    c = w["case"]
+    return c.conserved() if w["method"] == "weno" else c.dg_state(w["order"])
+
+
+def _ref_slabs(R, w, state, bct, nsteps, cores):
+    """(ms of the slowest slab, updated cells) for the reference's own
+    updateMesh run on `cores` x-slabs (threads standing in for MPI ranks)."""
+    c = w["case"]
+    if w["method"] == "weno":
+        return R.weno_slabs_timed(state, bct, c.da, c.gamma, w["dt"], nsteps, cores)
+    return R.dg_slabs_timed(w["order"], state, bct, c.da, c.gamma, w["dt"], nsteps, cores)
+
+
+def _ref_strip(R, w, cores, target_ms):
+    """A horizontal strip of the workload's grid sized so that one reference
+    step takes about target_ms on this host (bounded CPU sample)."""
+    c = w["case"]
+    full = _ref_state(w)
+    probe = min(c.ny, 64)
+    st = np.ascontiguousarray(full[..., :probe, :])
+    b = np.ascontiguousarray(c.bctype[:probe]).copy()
+    b[-3:] = -1
+    ms, _ = _ref_slabs(R, w, st, b, 1, cores)
+    rows = int(min(c.ny, max(16, probe * target_ms / max(ms, 1e-3))))
+    st = np.ascontiguousarray(full[..., :rows, :])
+    b = np.ascontiguousarray(c.bctype[:rows]).copy()
+    if rows < c.ny:
+        b[-3:] = -1
+    return st, b, rows
+
+
 def cpu_baseline(w: dict, seconds: float = 15.0) -> dict:
     """The reference's own sources (oracle/_ref, Makefile flags) on this host's
     cores: x-slab threads standing in for MPI ranks, a bounded sample."""
@@ -157,15 +213,14 @@ def cpu_baseline(w: dict, seconds: float = 15.0) -> dict:
     c = w["case"]
     cores = max(1, min(os.cpu_count() or 1, 64))
     R = Reference("faithful")
-    U = c.conserved()
-    # calibrate on one step, then run enough steps for ~`seconds` of work
-    ms, cells = R.weno_slabs_timed(U, c.bctype, c.da, c.gamma, w["dt"], 1, cores)
+    st, b, rows = _ref_strip(R, w, cores, 2000.0)
+    ms, cells = _ref_slabs(R, w, st, b, 1, cores)
     n = max(1, int(seconds * 1e3 / max(ms, 1.0)))
-    ms, cells = R.weno_slabs_timed(U, c.bctype, c.da, c.gamma, w["dt"], n, cores)
+    ms, cells = _ref_slabs(R, w, st, b, n, cores)
     v = cells * w["dof_per_cell"] * n / (ms * 1e-3)
     return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{n} x updateMesh on the full {c.ny}x{c.nx} grid split into {cores} x-slabs "
-                      f"(one thread per slab, reference Makefile flags, halo exchange omitted)",
+            "sample": f"{n} x updateMesh on a {rows}x{c.nx} strip of the {c.ny}x{c.nx} grid split into "
+                      f"{cores} x-slabs (one thread per slab, reference Makefile flags, halo exchange omitted)",
             "ms": ms}
 
 
@@ -176,15 +231,10 @@ def run_reference_arm(args, w) -> dict:
     c = w["case"]
     cores = max(1, min(os.cpu_count() or 1, 64))
     R = Reference("faithful")
-    U = c.conserved()
-    # bounded sample: a horizontal strip of the grid sized for <= ~1.5 s per step
-    ms1, _ = R.weno_slabs_timed(U[:, :256], c.bctype[:256], c.da, c.gamma, w["dt"], 1, cores)
-    rows = int(min(c.ny, max(64, 256 * 1500.0 / max(ms1, 1.0))))
-    Us, bs = np.ascontiguousarray(U[:, :rows]), np.ascontiguousarray(c.bctype[:rows]).copy()
-    bs[-3:] = -1
+    st, b, rows = _ref_strip(R, w, cores, 1500.0)
     for _ in range(args.warmup):
-        R.weno_slabs_timed(Us, bs, c.da, c.gamma, w["dt"], 1, cores)
-    ms, cells = R.weno_slabs_timed(Us, bs, c.da, c.gamma, w["dt"], args.steps, cores)
+        _ref_slabs(R, w, st, b, 1, cores)
+    ms, cells = _ref_slabs(R, w, st, b, args.steps, cores)
     v = cells * w["dof_per_cell"] * args.steps / (ms * 1e-3)
     sample = (f"{rows}x{c.nx} strip of the {c.ny}x{c.nx} grid per step, {cores} x-slab threads, "
               f"reference Makefile flags")
@@ -281,15 +331,24 @@ def main():
         peaks_file = ROOT / "MEASURED_PEAKS.json"
         hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
         roofs = {}
+        fl = FLOPS_PER_CELL_STAGE[(w["method"], w["order"])]
+        nvar = w["dof_per_cell"]
         for prec, pth in paths.items():
-            stage_ms = pth["ms"] / (3 * args.steps)  # every launch in a step is the stage kernel
-            achieved = cells * WENO_FLOPS_PER_CELL_STAGE / (stage_ms * 1e-3) / 1e12
+            stage_ms = pth["ms"] / (3 * args.steps)  # time of one RK stage (all its launches)
+            achieved = cells * fl / (stage_ms * 1e-3) / 1e12
             pk = peaks["fp64_tflops"] if prec == "fp64" else peaks["fp32_tflops"]
-            hbm_bytes = cells * 97.0  # FP64 state in + U^n + out + kind byte per stage (avg of 65/97/97)
+            # minimal traffic per stage: stage input + U^n + output (+ kind byte)
+            bpv = 8.0 if (prec == "fp64" or w["method"] == "weno") else 4.0
+            hbm_bytes = cells * (nvar * (bpv + 8.0 + bpv) + 1.0)
+            if w["method"] == "weno":
+                kname = "weno_stage_fp64_kernel" if prec == "fp64" else "weno_stage_mixed_kernel"
+            else:
+                kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if prec == "fp64"
+                         else "dg_stage_mixed_kernel")
             roofs[prec] = {
                 "bound": "fp64" if prec == "fp64" else "fp32", "achieved": achieved, "peak": pk,
                 "unit": "TFLOP/s", "frac": achieved / pk, "traffic": None,
-                "kernel": "weno_stage_fp64_kernel" if prec == "fp64" else "weno_stage_mixed_kernel",
+                "kernel": kname, "flops_per_cell_stage": fl,
                 "avg_launch_ms": stage_ms,
                 "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU "
                                "(MEASURED_PEAKS.json has no FP64/FP32 figure)",
@@ -307,7 +366,8 @@ def main():
                           "parallelism": f"replicas x{world} (independent seeded problems)"},
                "fp64_value": paths["fp64"]["value"],
                "speedup_vs_fp64": hp["value"] / paths["fp64"]["value"],
-               "clocks": hp["clocks"], "e2e": e2e, "gpu_launches": 3 * args.steps,
+               "clocks": hp["clocks"], "e2e": e2e,
+               "gpu_launches": 3 * args.steps if (w["method"] == "weno" or head == "mixed") else 9 * args.steps,
                "roofline": roofs[head], "roofline_fp64": roofs["fp64"], "cpu_baseline": cpu,
                "status_word": {p: v["status"] for p, v in paths.items()}, "peaks": peaks}
         print(json.dumps(out), flush=True)
@@ -319,7 +379,7 @@ def main():
 
 def open_solver(w, c, U0, precision, device):
     from zuikakucfd_b200 import Solver
-    s = Solver(method=w["method"], order=max(w["order"], 1), precision=precision, device=device)
+    s = Solver(method=w["method"], order=max(w["order"], 1), precision=precision, device=device, **w["opts"])
     s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
     s.set_state(U0)
     return s

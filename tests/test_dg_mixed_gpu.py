@@ -1,0 +1,96 @@
+"""GPU DG mixed-precision path (fused FP32 stage kernel, FP64 U^n
+accumulation, FP32 stage states) against the FP64 path, a finer FP64 solution
+(equal L1) and the exact translated wave."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def run(P, case, dt, steps, precision, boundary="exchange", flux="hllc", limiter="reference", state=None):
+    from zuikakucfd_b200 import Solver
+    with Solver(method="dg", order=P, precision=precision, boundary=boundary, flux=flux, limiter=limiter) as s:
+        s.set_mesh(case.ny, case.nx, case.da, case.gamma, case.bctype)
+        s.set_state(case.dg_state(P) if state is None else state)
+        s.step(dt, steps)
+        return s.get_state(), s.status_word()
+
+
+def dg_dt(P, case, cfl_frac=0.5):
+    lam = case.da / __import__("zuikakucfd_b200").cases.cfl_dt(case, 1.0)
+    return cfl_frac * 0.9 / (2.0 * (2 * P + 1)) * case.da / lam
+
+
+@pytest.mark.parametrize("P", [1, 2, 3])
+def test_mixed_tracks_fp64(P):
+    from zuikakucfd_b200 import cases
+    c = cases.four_quadrant(70, seed=3, ny=45)    # odd sizes: partial tiles
+    dt = dg_dt(P, c)
+    f64, s1 = run(P, c, dt, 20, "fp64")
+    mix, s2 = run(P, c, dt, 20, "mixed")
+    assert s1 == 0 and s2 == 0
+    assert np.isfinite(mix).all()
+    for q in range(4):
+        d = np.abs(mix[q, 0] - f64[q, 0]).sum() / np.abs(f64[q, 0]).sum()
+        assert d < 2e-5, (q, d)
+
+
+@pytest.mark.parametrize("P", [1, 2, 3])
+def test_mixed_hll_and_no_limiter(P):
+    from zuikakucfd_b200 import cases
+    c = cases.four_quadrant(40, seed=6)
+    dt = dg_dt(P, c, 0.3)
+    for flux, lim in (("hll", "reference"), ("hllc", "none")):
+        f64, _ = run(P, c, dt, 10, "fp64", flux=flux, limiter=lim)
+        mix, st = run(P, c, dt, 10, "mixed", flux=flux, limiter=lim)
+        d = np.abs(mix[0, 0] - f64[0, 0]).sum() / np.abs(f64[0, 0]).sum()
+        assert d < 2e-5, (flux, lim, d)
+
+
+def _restrict(a, f):
+    x = a[3:-3, 3:-3]
+    n0, n1 = x.shape[0] // f, x.shape[1] // f
+    return x.reshape(n0, f, n1, f).mean(axis=(1, 3))
+
+
+@pytest.mark.parametrize("P", [2, 3])
+def test_mixed_equal_l1_against_finer_fp64(P):
+    """Four-quadrant Riemann problem: 64^2 coarse vs 256^2 FP64 reference (cell
+    averages restricted), same physical time.  Mixed L1 <= 1.1 x FP64 L1."""
+    from zuikakucfd_b200 import cases
+    f = 4
+    cc = cases.four_quadrant(64, seed=2, ring_outside=True)
+    cf = cases.four_quadrant(64 * f, seed=2, ring_outside=True)
+    t_end = 0.05
+    dtc = dg_dt(P, cc, 0.8)
+    n = int(np.ceil(t_end / dtc))
+    dtc = t_end / n
+    ref, st = run(P, cf, dtc / f, n * f, "fp64")
+    assert st == 0
+    rho_ref = _restrict(ref[0, 0], f)
+    a64, _ = run(P, cc, dtc, n, "fp64")
+    amx, _ = run(P, cc, dtc, n, "mixed")
+    e64 = np.abs(a64[0, 0, 3:-3, 3:-3] - rho_ref).mean()
+    emx = np.abs(amx[0, 0, 3:-3, 3:-3] - rho_ref).mean()
+    assert emx <= 1.1 * e64, (emx, e64)
+
+
+def test_mixed_smooth_wave_against_exact():
+    """DG P=2 periodic smooth wave at 64^2 to t=0.2: the mixed path's L1 error
+    against the exact translated density is within 1.1x the FP64 path's."""
+    from zuikakucfd_b200 import cases
+    w = cases.smooth_wave(64)
+    P = 2
+    dt0 = 0.09 * w.da / 2.74
+    t_end = 0.2
+    n = int(np.ceil(t_end / dt0))
+    dt = t_end / n
+    # exact cell average of the translated wave (sin averages over a square by sinc^2)
+    kh = np.pi * w.da / 2.0
+    ex = 1.0 + (cases.smooth_wave_exact(w, t_end) - 1.0) * (np.sin(kh) / kh) ** 2
+    errs = {}
+    for prec in ("fp64", "mixed"):
+        out, st = run(P, w, dt, n, prec, boundary="periodic", limiter="none")
+        assert st == 0
+        errs[prec] = np.abs(out[0, 0, 3:-3, 3:-3] - ex).mean()
+    assert errs["mixed"] <= 1.1 * errs["fp64"], errs

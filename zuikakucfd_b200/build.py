@@ -38,6 +38,7 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("reduce_fp64.cu", STRICT),
     ("dg_fp64.cu", STRICT),
     ("dg_driver.cu", []),
+    ("dg_mixed.cu", ["--use_fast_math"]),
     ("peak.cu", []),
     ("weno_mixed.cu", ["--use_fast_math"]),
     ("noalloc.cu", []),

@@ -8,6 +8,11 @@
 namespace zk {
 cudaError_t launch_dg_stage_fp64(int P, const DGArgs& a, cudaStream_t s);
 cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s);
+int dg_upload_tables_f32(int P);
+cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
+                                  const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
+                                  double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
+                                  cudaStream_t s);
 }  // namespace zk
 
 namespace {
@@ -49,8 +54,6 @@ int cuda_fail(cudaError_t e) { return zk_internal_fail(ZK_ERR_CUDA, cudaGetError
 
 int zk_dg_setup(zk_ctx* c) {
     const int P = c->opt.order;
-    if (c->opt.precision != ZK_PREC_FP64)
-        return zk_internal_fail(ZK_ERR_UNSUPPORTED, "DG mixed precision is not available in this build");
     if (c->opt.limiter != ZK_LIMITER_REFERENCE && c->opt.limiter != ZK_LIMITER_NONE)
         return zk_internal_fail(ZK_ERR_UNSUPPORTED, "DG TVB limiters are not available in this build");
     DGState* s = new DGState();
@@ -67,6 +70,14 @@ int zk_dg_setup(zk_ctx* c) {
         e = cudaMemcpyAsync(c->d_phic, phic, sizeof(double) * NM * 4, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMalloc(&s->fx, sizeof(double) * NQ * 4 * (size_t)c->g.ny * s->xpitch);
     if (e == cudaSuccess) e = cudaMalloc(&s->fy, sizeof(double) * NQ * 4 * (size_t)(c->g.ny + 1) * c->g.pitch);
+    if (e == cudaSuccess && c->opt.precision == ZK_PREC_MIXED) {
+        if (zk::dg_upload_tables_f32(P) != ZK_OK) return zk_internal_fail(ZK_ERR_CUDA, "DG FP32 table upload failed");
+        const size_t n = (size_t)4 * NM * c->g.plane;
+        e = cudaMalloc(&c->F1, sizeof(float) * n);
+        if (e == cudaSuccess) e = cudaMalloc(&c->F2, sizeof(float) * n);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->F1, 0, sizeof(float) * n, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->F2, 0, sizeof(float) * n, c->stream);
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }
@@ -80,7 +91,22 @@ void zk_dg_release(zk_ctx* c) {
     c->dg = nullptr;
 }
 
+static int dg_step_mixed(zk_ctx* c, double dt) {
+    const int P = c->opt.order, lim = c->opt.limiter, hll = c->opt.flux == ZK_FLUX_HLL;
+    const double s0 = st(c)->s0;
+    cudaError_t e = zk::launch_dg_stage_mixed(P, c->Un, 1, c->Un, c->F1, 0, c->kind, c->gsrc, c->g, dt, c->da,
+                                              c->gamma, 1, lim, hll, s0, c->d_status, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_dg_stage_mixed(P, c->F1, 0, c->Un, c->F2, 0, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 2,
+                                      lim, hll, s0, c->d_status, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_dg_stage_mixed(P, c->F2, 0, c->Un, c->Un, 1, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 3,
+                                      lim, hll, s0, c->d_status, c->stream);
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
 int zk_dg_step(zk_ctx* c, double dt) {
+    if (c->opt.precision == ZK_PREC_MIXED) return dg_step_mixed(c, dt);
     const int P = c->opt.order;
     cudaError_t e = zk::launch_dg_stage_fp64(P, args(c, c->Un, c->Un, c->S1, dt, 1), c->stream);
     if (e == cudaSuccess) e = zk::launch_dg_stage_fp64(P, args(c, c->S1, c->Un, c->S2, dt, 2), c->stream);

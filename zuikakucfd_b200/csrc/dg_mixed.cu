@@ -1,0 +1,516 @@
+// DG P=1..3 stage, mixed precision, ONE fused kernel per RK stage.
+//
+// A CTA owns a 32 x 4 tile of cells.  It gathers the tile plus a 1-cell halo
+// of the stage input into shared memory as FP32 (ghosts through the fill
+// source map, slip walls negated), computes every interface flux of the tile
+// once from the two cells' traces (FP32, in shared memory), then each thread
+// runs its cell's volume quadrature and face integrals in FP32 registers.
+// The Shu-Osher combine is FP64 against the FP64 U^n; the Persson +
+// Zhang-Shu limiter decides in FP32 and is applied as per-mode factors to the
+// FP64 combine.  Stage states U^(1), U^(2) are stored in FP32, U^(n+1) in
+// FP64.  This file is compiled with --use_fast_math (FP32 division, sqrt,
+// log10 and sin use the MUFU approximations).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "dg_common.cuh"
+#include "zk_internal.h"
+
+namespace zk {
+namespace {
+
+struct DGTabF {
+    float vw[DG_MAXNQ * DG_MAXNQ];
+    float vphi[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];
+    float vdxi[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];
+    float vdet[DG_MAXNQ * DG_MAXNQ][DG_MAXNM];
+    float tr[4][DG_MAXNQ][DG_MAXNM];
+    float bv[4][DG_MAXNQ][DG_MAXNM];
+    float zs[16][DG_MAXNM];
+};
+
+__constant__ DGTabF c_tabf[3];
+
+constexpr int MTX = 32, MTY = 4, MNT = MTX * MTY;
+constexpr int SX = MTX + 2, SY = MTY + 2;  // tile + 1-cell halo
+
+struct MixArgs {
+    const void* cur;  // stage input: double (stage 1: U^n) or float (U^(1), U^(2))
+    const double* un;
+    void* out;        // float (stages 1, 2) or double (stage 3)
+    const int8_t* kind;
+    const int32_t* gsrc;
+    Grid g;
+    double dt;
+    float inv2h, gamma;
+    int stage, limiter, hll;
+    float s0;
+    uint32_t* status;
+};
+
+__device__ __forceinline__ float fmaxr(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float fminr(float a, float b) { return (b < a) ? b : a; }
+
+// eulerFluxX/Y (src_DG/fluid.cpp:123-143), FP32
+__device__ __forceinline__ void euler_flux_f(const float U[4], float gam, float F[4], float G[4]) {
+    const float eps = 1e-3f;
+    float rho = fmaxr(U[0], eps);
+    float ir = 1.0f / rho;
+    float u = U[1] * ir, v = U[2] * ir;
+    float p = fmaxr((gam - 1.0f) * (U[3] - 0.5f * rho * (u * u + v * v)), eps);
+    F[0] = rho * u; F[1] = rho * u * u + p; F[2] = rho * u * v; F[3] = (U[3] + p) * u;
+    G[0] = rho * v; G[1] = rho * u * v; G[2] = rho * v * v + p; G[3] = (U[3] + p) * v;
+}
+
+// hllcFlux DG variant (src_DG/fluid.cpp:450-520), FP32
+__device__ __forceinline__ void hllc_dg_f(const float L[4], const float R[4], float gamma, float F[4]) {
+    const float eps = 1e-5f;
+    float rhoL = fmaxr(L[0], eps), irL = 1.0f / rhoL, uL = L[1] * irL, vL = L[2] * irL;
+    float pL = fmaxr((gamma - 1.0f) * (L[3] - 0.5f * rhoL * (uL * uL + vL * vL)), eps);
+    float aL = sqrtf(fmaxr(gamma * pL * irL, eps));
+    float rhoR = fmaxr(R[0], eps), irR = 1.0f / rhoR, uR = R[1] * irR, vR = R[2] * irR;
+    float pR = fmaxr((gamma - 1.0f) * (R[3] - 0.5f * rhoR * (uR * uR + vR * vR)), eps);
+    float aR = sqrtf(fmaxr(gamma * pR * irR, eps));
+    float sqL = sqrtf(rhoL), sqR = sqrtf(rhoR);
+    float den = sqL + sqR;
+    if (den < eps) den = eps;
+    float iden = 1.0f / den;
+    float u_roe = (sqL * uL + sqR * uR) * iden;
+    float h_roe = (sqL * ((L[3] + pL) * irL) + sqR * ((R[3] + pR) * irR)) * iden;
+    float c_roe = sqrtf(fmaxr((gamma - 1.0f) * (h_roe - 0.5f * u_roe * u_roe), eps));
+    float SL = fminr(uL - aL, u_roe - c_roe);
+    float SR = fmaxr(uR + aR, u_roe + c_roe);
+    if (SL >= 0.0f) {
+        F[0] = rhoL * uL; F[1] = rhoL * uL * uL + pL; F[2] = rhoL * uL * vL; F[3] = (L[3] + pL) * uL;
+        return;
+    }
+    if (SR <= 0.0f) {
+        F[0] = rhoR * uR; F[1] = rhoR * uR * uR + pR; F[2] = rhoR * uR * vR; F[3] = (R[3] + pR) * uR;
+        return;
+    }
+    float num = pR - pL + rhoL * uL * (SL - uL) - rhoR * uR * (SR - uR);
+    float den2 = rhoL * (SL - uL) - rhoR * (SR - uR);
+    if (fabsf(den2) < eps) den2 = (den2 >= 0.0f ? eps : -eps);
+    float Ss = num / den2;
+    const bool left = Ss >= 0.0f;
+    const float rho = left ? rhoL : rhoR, u = left ? uL : uR, v = left ? vL : vR;
+    const float p = left ? pL : pR, S = left ? SL : SR, ir = left ? irL : irR;
+    const float* Us = left ? L : R;
+    float denom = S - Ss;
+    if (fabsf(denom) < eps) denom = (denom >= 0.0f ? eps : -eps);
+    float c = rho * (S - u) / denom;
+    float term = (Ss - u) * (Ss + p / (rho * (S - u)));
+    if (!isfinite(term)) term = 0.0f;
+    F[0] = rho * u + S * (c - Us[0]);
+    F[1] = rho * u * u + p + S * (c * Ss - Us[1]);
+    F[2] = rho * u * v + S * (c * v - Us[2]);
+    F[3] = (Us[3] + p) * u + S * (c * (Us[3] * ir + term) - Us[3]);
+}
+
+// hlleFlux (src_DG/fluid.cpp:525-580), FP32
+__device__ __forceinline__ void hlle_dg_f(const float L[4], const float R[4], float gamma, float F[4]) {
+    const float eps = 1e-6f;
+    float rhoL = fmaxr(L[0], eps), irL = 1.0f / rhoL, uL = L[1] * irL, vL = L[2] * irL, EL = L[3];
+    float pL = fmaxr((gamma - 1.0f) * (EL - 0.5f * rhoL * (uL * uL + vL * vL)), eps);
+    float aL = sqrtf(fmaxr(gamma * pL * irL, eps));
+    float rhoR = fmaxr(R[0], eps), irR = 1.0f / rhoR, uR = R[1] * irR, vR = R[2] * irR, ER = R[3];
+    float pR = fmaxr((gamma - 1.0f) * (ER - 0.5f * rhoR * (uR * uR + vR * vR)), eps);
+    float aR = sqrtf(fmaxr(gamma * pR * irR, eps));
+    float sqL = sqrtf(rhoL), sqR = sqrtf(rhoR);
+    float invDen = 1.0f / fmaxr(sqL + sqR, eps);
+    float u_roe = (sqL * uL + sqR * uR) * invDen, v_roe = (sqL * vL + sqR * vR) * invDen;
+    float h_roe = (sqL * ((EL + pL) * irL) + sqR * ((ER + pR) * irR)) * invDen;
+    float c_roe = sqrtf(fmaxr((gamma - 1.0f) * (h_roe - 0.5f * (u_roe * u_roe + v_roe * v_roe)), eps));
+    float SL = fminr(uL - aL, u_roe - c_roe), SR = fmaxr(uR + aR, u_roe + c_roe);
+    float FL[4] = {rhoL * uL, rhoL * uL * uL + pL, rhoL * uL * vL, (EL + pL) * uL};
+    float FR[4] = {rhoR * uR, rhoR * uR * uR + pR, rhoR * uR * vR, (ER + pR) * uR};
+    if (SL >= 0.0f) {
+        for (int c = 0; c < 4; ++c) F[c] = FL[c];
+    } else if (SR <= 0.0f) {
+        for (int c = 0; c < 4; ++c) F[c] = FR[c];
+    } else {
+        float invDiff = 1.0f / fmaxr(SR - SL, eps);
+        for (int c = 0; c < 4; ++c) F[c] = (SR * FL[c] - SL * FR[c] + SL * SR * (R[c] - L[c])) * invDiff;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ float load_f(const void* p, size_t i) {
+    return (float)static_cast<const T*>(p)[i];
+}
+
+template <int P, typename TIn, typename TOut>
+__global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
+    constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
+    constexpr int SD = SX * SY;  // slots of one plane
+    const DGTabF& T = c_tabf[P - 1];
+    extern __shared__ __align__(16) float smem[];
+    float* sd = smem;                       // [4*NM][SY][SX] gathered stage input
+    float* sfx = sd + 4 * NM * SD;          // [NQ*4][MTY][MTX+1]
+    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
+
+    const int tid = threadIdx.x;
+    const int j0 = blockIdx.x * MTX, i0 = blockIdx.y * MTY;
+    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
+    const size_t plane = a.g.plane;
+
+    // 0. gather tile + halo (corners unused)
+    for (int slot = tid; slot < SD; slot += MNT) {
+        const int r = slot / SX, c = slot - r * SX;
+        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        uint8_t kd = KIND_PASSIVE;
+        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+            const size_t k = (size_t)gi * pitch + gj;
+            kd = a.kind[k] & KIND_MASK;
+            size_t ks = k;
+            int neg = -1;
+            if (kd >= KIND_COPY) {
+                ks = (size_t)a.gsrc[k];
+                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
+            }
+#pragma unroll 4
+            for (int v = 0; v < 4 * NM; ++v) {
+                const float x = load_f<TIn>(a.cur, (size_t)v * plane + ks);
+                sd[v * SD + slot] = (neg == v / NM) ? -x : x;
+            }
+        } else {
+            for (int v = 0; v < 4 * NM; ++v) sd[v * SD + slot] = 0.0f;
+        }
+        sk[slot] = kd;
+    }
+    __syncthreads();
+
+    // 1. interface fluxes of the tile, once each
+    constexpr int NXF = MTY * (MTX + 1), NYF = (MTY + 1) * MTX;
+    for (int f = tid; f < NXF + NYF; f += MNT) {
+        int sl, sr, side_l, side_r;
+        float* dst;
+        int dstride;
+        bool ydir;
+        if (f < NXF) {
+            const int r = f / (MTX + 1), c = f - r * (MTX + 1);
+            sl = (r + 1) * SX + c;          // left cell slot
+            sr = sl + 1;                     // right cell slot
+            side_l = 0; side_r = 1;          // xi=+1 of left, xi=-1 of right
+            dst = sfx + r * (MTX + 1) + c;
+            dstride = MTY * (MTX + 1);
+            ydir = false;
+        } else {
+            const int g = f - NXF, r = g / MTX, c = g - r * MTX;
+            sl = r * SX + c + 1;             // cell above
+            sr = sl + SX;                    // cell below
+            side_l = 2; side_r = 3;          // eta=+1 of upper, eta=-1 of lower
+            dst = sfy + r * MTX + c;
+            dstride = (MTY + 1) * MTX;
+            ydir = true;
+        }
+        if (sk[sl] != KIND_UPDATED && sk[sr] != KIND_UPDATED) continue;
+        float UL[NQ][4], UR[NQ][4];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) UL[q][c] = UR[q][c] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float dl = sd[(c * NM + m) * SD + sl], dr = sd[(c * NM + m) * SD + sr];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    UL[q][c] = fmaf(dl, T.tr[side_l][q][m], UL[q][c]);
+                    UR[q][c] = fmaf(dr, T.tr[side_r][q][m], UR[q][c]);
+                }
+            }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            float Fq[4];
+            if (ydir) {
+                float l[4] = {UL[q][0], UL[q][2], UL[q][1], UL[q][3]};
+                float r[4] = {UR[q][0], UR[q][2], UR[q][1], UR[q][3]};
+                float g[4];
+                if (a.hll) hlle_dg_f(l, r, a.gamma, g);
+                else hllc_dg_f(l, r, a.gamma, g);
+                Fq[0] = g[0]; Fq[1] = g[2]; Fq[2] = g[1]; Fq[3] = g[3];
+            } else {
+                if (a.hll) hlle_dg_f(UL[q], UR[q], a.gamma, Fq);
+                else hllc_dg_f(UL[q], UR[q], a.gamma, Fq);
+            }
+#pragma unroll
+            for (int c = 0; c < 4; ++c) dst[(q * 4 + c) * dstride] = Fq[c];
+        }
+    }
+    __syncthreads();
+
+    // 2. one thread per cell
+    const int r = tid / MTX, c = tid - r * MTX;
+    const int gi = i0 + r, gj = j0 + c;
+    if (gi >= ny || gj >= nx) return;
+    const int slot = (r + 1) * SX + c + 1;
+    const size_t k = (size_t)gi * pitch + gj;
+    const uint8_t kd = sk[slot];
+    float acc[4][NM];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[q][m] = 0.0f;
+    if (kd == KIND_UPDATED) {
+#pragma unroll 1
+        for (int p = 0; p < NV; ++p) {
+            float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const float b = T.vphi[p][m];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) U[q] = fmaf(sd[(q * NM + m) * SD + slot], b, U[q]);
+            }
+            float F[4], G[4];
+            euler_flux_f(U, a.gamma, F, G);
+            const float w = T.vw[p];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { F[q] *= w; G[q] *= w; }
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const float dxi = T.vdxi[p][m], det = T.vdet[p][m];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q][m] = fmaf(F[q], dxi, fmaf(G[q], det, acc[q][m]));
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+            const float* Fb = (f == 0) ? sfx + r * (MTX + 1) + c + 1
+                            : (f == 1) ? sfx + r * (MTX + 1) + c
+                            : (f == 2) ? sfy + (r + 1) * MTX + c
+                                       : sfy + r * MTX + c;
+            const int fs = (f < 2) ? MTY * (MTX + 1) : (MTY + 1) * MTX;
+            const float sgn = (f == 0 || f == 2) ? -1.0f : 1.0f;
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) {
+                float Fs[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) Fs[u] = sgn * Fb[(q * 4 + u) * fs];
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const float bv = T.bv[f][q][m];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u][m] = fmaf(bv, Fs[u], acc[u][m]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+            const float scale = (float)((2 * (m / NQ) + 1) * (2 * (m % NQ) + 1)) * a.inv2h;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q][m] *= scale;
+        }
+    }
+
+    if (a.stage == 0) {
+#pragma unroll
+        for (int v = 0; v < 4 * NM; ++v) static_cast<TOut*>(a.out)[(size_t)v * plane + k] = (TOut)acc[v / NM][v % NM];
+        return;
+    }
+    // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
+    const double dt = a.dt;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+            const int v = q * NM + m;
+            const double un = a.un[(size_t)v * plane + k];
+            const double dd = dt * (double)acc[q][m];
+            double o;
+            if (a.stage == 1) {
+                o = un + dd;
+            } else {
+                const double w = (double)sd[v * SD + slot] + dd;
+                sd[v * SD + slot] = (float)w;  // own slot: no other thread reads it any more
+                o = (a.stage == 2) ? 0.75 * un + 0.25 * w : (1.0 / 3.0) * un + (2.0 / 3.0) * w;
+            }
+            acc[q][m] = (float)o;
+        }
+
+    // limiter decisions in FP32 (src_DG/fluid.cpp:824-992), as factors
+    float pf[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+    float theta = 1.0f;
+    bool rho_clamp = false, e_fix = false;
+    const bool in_range = gi >= 3 && gi < ny - 3 && gj >= 3 && gj < nx - 3;
+    if (a.limiter == ZK_LIMITER_REFERENCE && in_range) {
+        if (kd == KIND_UPDATED) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                float Et = 0.0f, Ep = 0.0f;
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const float x = acc[q][m] * acc[q][m];
+                    Et += x;
+                    if (m / NQ == P || m % NQ == P) Ep += x;
+                }
+                const float s = log10f(Ep / (Et + 1e-5f));
+                if (s > a.s0) {
+                    const float eps = (s > a.s0 + 1.0f) ? 1.0f : 0.5f * (1.0f + sinf(3.14159265f * ((s - a.s0) - 0.5f)));
+                    pf[q] = 1.0f - eps;
+#pragma unroll
+                    for (int m = 0; m < NM; ++m)
+                        if (m / NQ == P || m % NQ == P) acc[q][m] *= pf[q];
+                }
+            }
+        }
+        const float RHO_MIN = 1e-5f, P_MIN = 1e-5f, EPS = 1e-5f, g1 = a.gamma - 1.0f;
+        if (acc[0][0] < RHO_MIN) { acc[0][0] = RHO_MIN; rho_clamp = true; }
+        const float rho0 = acc[0][0], mx0 = acc[1][0], my0 = acc[2][0];
+        const float ke0 = 0.5f * (mx0 * mx0 + my0 * my0) / rho0;
+        if (g1 * (acc[3][0] - ke0) < P_MIN) { acc[3][0] = P_MIN / g1 + ke0; e_fix = true; }
+        float th = 1.0f;
+#pragma unroll 1
+        for (int pt = 0; pt < 16; ++pt) {
+            float rho = 0.0f;
+#pragma unroll
+            for (int m = 0; m < NM; ++m) rho = fmaf(acc[0][m], T.zs[pt][m], rho);
+            if (rho < RHO_MIN) th = fminr(th, (rho0 - RHO_MIN) / (rho0 - rho + EPS));
+        }
+        if (th < 1.0f) {
+#pragma unroll
+            for (int m = 1; m < NM; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q][m] *= th;
+        }
+        const float p_avg = g1 * (acc[3][0] - 0.5f * (acc[1][0] * acc[1][0] + acc[2][0] * acc[2][0]) / acc[0][0]);
+        float tp = 1.0f;
+#pragma unroll 1
+        for (int pt = 0; pt < 16; ++pt) {
+            float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const float phi = T.zs[pt][m];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) U[q] = fmaf(acc[q][m], phi, U[q]);
+            }
+            if (U[0] <= RHO_MIN) continue;
+            const float p = g1 * (U[3] - 0.5f * (U[1] * U[1] + U[2] * U[2]) / U[0]);
+            if (p < P_MIN) tp = fminr(tp, (p_avg - P_MIN) / (p_avg - p + EPS));
+        }
+        if (tp < 1.0f) {
+#pragma unroll
+            for (int m = 1; m < NM; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q][m] *= tp;
+        }
+        theta = th * tp;
+    }
+
+    uint32_t flags = 0;
+    if (kd == KIND_UPDATED) {
+        if (!isfinite(acc[0][0]) || !isfinite(acc[3][0])) flags |= STATUS_NAN;
+        if (!(acc[0][0] > 0.0f)) flags |= STATUS_RHO;
+    }
+    TOut* out = static_cast<TOut*>(a.out);
+    if (sizeof(TOut) == 4) {
+#pragma unroll
+        for (int v = 0; v < 4 * NM; ++v) out[(size_t)v * plane + k] = (TOut)acc[v / NM][v % NM];
+    } else {
+        // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
+        double e0 = 0.0;
+        if (e_fix) {
+            const double rho0 = rho_clamp ? 1e-5 : (1.0 / 3.0) * a.un[k] + (2.0 / 3.0) * (double)sd[slot];
+            const double mx0 = (1.0 / 3.0) * a.un[(size_t)NM * plane + k] + (2.0 / 3.0) * (double)sd[NM * SD + slot];
+            const double my0 = (1.0 / 3.0) * a.un[(size_t)2 * NM * plane + k] + (2.0 / 3.0) * (double)sd[2 * NM * SD + slot];
+            e0 = 1e-5 / (double)(a.gamma - 1.0f) + 0.5 * (mx0 * mx0 + my0 * my0) / rho0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const int v = q * NM + m;
+                double o = (1.0 / 3.0) * a.un[(size_t)v * plane + k] + (2.0 / 3.0) * (double)sd[v * SD + slot];
+                if (m == 0) {
+                    if (q == 0 && rho_clamp) o = 1e-5;
+                    if (q == 3 && e_fix) o = e0;
+                } else {
+                    if (m / NQ == P || m % NQ == P) o *= (double)pf[q];
+                    o *= (double)theta;
+                }
+                out[(size_t)v * plane + k] = (TOut)o;
+            }
+        if (kd == KIND_UPDATED) {
+            const double rho = out[k], mx = out[(size_t)NM * plane + k], my = out[(size_t)2 * NM * plane + k];
+            const double p = (double)(a.gamma - 1.0f) * (out[(size_t)3 * NM * plane + k] - 0.5 * (mx * mx + my * my) / rho);
+            if (!(p > 0.0)) flags |= STATUS_P;
+        }
+    }
+    if (flags) atomicOr(a.status, flags);
+}
+
+template <int P>
+constexpr size_t smem_bytes() {
+    constexpr int NQ = P + 1, NM = NQ * NQ;
+    return sizeof(float) * (4 * NM * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
+}
+
+template <int P, typename TIn, typename TOut>
+cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
+    constexpr size_t sm = smem_bytes<P>();
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(dg_stage_mixed_kernel<P, TIn, TOut>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY);
+    dg_stage_mixed_kernel<P, TIn, TOut><<<grid, MNT, sm, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int P>
+cudaError_t launch_p(const MixArgs& a, int in_fp64, int out_fp64, cudaStream_t s) {
+    if (in_fp64 && !out_fp64) return launch_one<P, double, float>(a, s);
+    if (!in_fp64 && !out_fp64) return launch_one<P, float, float>(a, s);
+    if (!in_fp64 && out_fp64) return launch_one<P, float, double>(a, s);
+    return launch_one<P, double, double>(a, s);
+}
+
+}  // namespace
+
+// FP32 copy of P's basis tables in this file's constant bank (once per device, P).
+int dg_upload_tables_f32(int P) {
+    static std::mutex mu;
+    static uint64_t done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return ZK_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev] & (1ull << P)) return ZK_OK;
+    DGTab T;
+    double phic[DG_MAXNM * 4];
+    dg_make_tables(P, &T, phic);
+    DGTabF F;
+    std::memset(&F, 0, sizeof F);
+    const double* src = reinterpret_cast<const double*>(&T);
+    float* dst = reinterpret_cast<float*>(&F);
+    static_assert(sizeof(DGTab) / sizeof(double) == sizeof(DGTabF) / sizeof(float), "table layouts differ");
+    for (size_t i = 0; i < sizeof(DGTab) / sizeof(double); ++i) dst[i] = (float)src[i];
+    if (cudaMemcpyToSymbol(c_tabf, &F, sizeof F, sizeof F * (P - 1)) != cudaSuccess) return ZK_ERR_CUDA;
+    done[dev] |= (1ull << P);
+    return ZK_OK;
+}
+
+// One mixed-precision DG stage: cur (double if in_fp64 else float) -> out
+// (double if out_fp64 else float).
+cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
+                                  const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
+                                  double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
+                                  cudaStream_t s) {
+    MixArgs a{cur, un, out, kind, gsrc, g, dt, (float)(0.5 / da), (float)gamma, stage, limiter, hll, (float)s0,
+              status};
+    switch (P) {
+        case 1: return launch_p<1>(a, in_fp64, out_fp64, s);
+        case 2: return launch_p<2>(a, in_fp64, out_fp64, s);
+        case 3: return launch_p<3>(a, in_fp64, out_fp64, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace zk
