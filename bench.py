@@ -55,10 +55,11 @@ def make_workload(name: str, rank: int):
         dt = 0.003 * c.da / (30.0 + float(np.sqrt(c.gamma * 0.4127 / 5.0)))
         return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=dt, opts={},
                     desc="high-Mach jet 2048x1024 (rho=5,u=30 band, gamma=5/3), WENO5+HLLC+SSP-RK3, CFL 0.003")
-    if name == "weno_fq_2048":
-        c = cases.four_quadrant(2048, seed=seed)
+    if name.startswith("weno_fq_"):
+        n = int(name.split("_")[-1])
+        c = cases.four_quadrant(n, seed=seed)
         return dict(case=c, method="weno", order=0, dof_per_cell=4, dt=cases.cfl_dt(c, 0.4), opts={},
-                    desc=f"seeded four-quadrant Riemann 2048x2048 (seed {seed}), WENO5+HLLC+SSP-RK3, CFL 0.4")
+                    desc=f"seeded four-quadrant Riemann {n}x{n} (seed {seed}), WENO5+HLLC+SSP-RK3, CFL 0.4")
     if name.startswith("dg") and "_fq_" in name:
         P = int(name[2])
         n = int(name.split("_")[-1])

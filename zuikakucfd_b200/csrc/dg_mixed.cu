@@ -135,19 +135,24 @@ __device__ __forceinline__ void hlle_dg_f(const float L[4], const float R[4], fl
     }
 }
 
+// Floats per cell slot in shared memory: 4*NM rounded so that (stride/4) is
+// odd, which puts 8 consecutive cells' 16-byte loads in 8 distinct bank groups.
+__host__ __device__ constexpr int vpitch(int nm) { return ((4 * nm / 4) % 2 == 1) ? 4 * nm : 4 * nm + 4; }
+
 template <typename T>
 __device__ __forceinline__ float load_f(const void* p, size_t i) {
     return (float)static_cast<const T*>(p)[i];
 }
 
 template <int P, typename TIn, typename TOut>
-__global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
+__global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
-    constexpr int SD = SX * SY;  // slots of one plane
+    constexpr int SD = SX * SY;  // cell slots of the tile + halo
+    constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
     const DGTabF& T = c_tabf[P - 1];
     extern __shared__ __align__(16) float smem[];
-    float* sd = smem;                       // [4*NM][SY][SX] gathered stage input
-    float* sfx = sd + 4 * NM * SD;          // [NQ*4][MTY][MTX+1]
+    float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
+    float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
     float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
     uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
 
@@ -170,13 +175,22 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
                 ks = (size_t)a.gsrc[k];
                 neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
             }
-#pragma unroll 4
-            for (int v = 0; v < 4 * NM; ++v) {
-                const float x = load_f<TIn>(a.cur, (size_t)v * plane + ks);
-                sd[v * SD + slot] = (neg == v / NM) ? -x : x;
+#pragma unroll 2
+            for (int v = 0; v < 4 * NM; v += 4) {
+                float4 x;
+                x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
+                x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
+                x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
+                x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
+                if (neg == (v + 0) / NM) x.x = -x.x;
+                if (neg == (v + 1) / NM) x.y = -x.y;
+                if (neg == (v + 2) / NM) x.z = -x.z;
+                if (neg == (v + 3) / NM) x.w = -x.w;
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
             }
         } else {
-            for (int v = 0; v < 4 * NM; ++v) sd[v * SD + slot] = 0.0f;
+            for (int v = 0; v < 4 * NM; v += 4)
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
         sk[slot] = kd;
     }
@@ -212,17 +226,23 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
         for (int q = 0; q < NQ; ++q)
 #pragma unroll
             for (int c = 0; c < 4; ++c) UL[q][c] = UR[q][c] = 0.0f;
+        const float* pl = sd + sl * VP;
+        const float* pr = sd + sr * VP;
 #pragma unroll
-        for (int m = 0; m < NM; ++m)
+        for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
+            const float4 l4 = *reinterpret_cast<const float4*>(pl + v4);
+            const float4 r4 = *reinterpret_cast<const float4*>(pr + v4);
+            const float lv[4] = {l4.x, l4.y, l4.z, l4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float dl = sd[(c * NM + m) * SD + sl], dr = sd[(c * NM + m) * SD + sr];
+            for (int e = 0; e < 4; ++e) {
+                const int c = (v4 + e) / NM, m = (v4 + e) % NM;
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
-                    UL[q][c] = fmaf(dl, T.tr[side_l][q][m], UL[q][c]);
-                    UR[q][c] = fmaf(dr, T.tr[side_r][q][m], UR[q][c]);
+                    UL[q][c] = fmaf(lv[e], T.tr[side_l][q][m], UL[q][c]);
+                    UR[q][c] = fmaf(rv[e], T.tr[side_r][q][m], UR[q][c]);
                 }
             }
+        }
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
             float Fq[4];
@@ -256,14 +276,17 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
 #pragma unroll
         for (int m = 0; m < NM; ++m) acc[q][m] = 0.0f;
     if (kd == KIND_UPDATED) {
-#pragma unroll 1
+        const float* pc = sd + slot * VP;
+#pragma unroll
         for (int p = 0; p < NV; ++p) {
             float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                const float b = T.vphi[p][m];
+            for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
+                const float4 d4 = *reinterpret_cast<const float4*>(pc + v4);
+                const float dv[4] = {d4.x, d4.y, d4.z, d4.w};
 #pragma unroll
-                for (int q = 0; q < 4; ++q) U[q] = fmaf(sd[(q * NM + m) * SD + slot], b, U[q]);
+                for (int e = 0; e < 4; ++e)
+                    U[(v4 + e) / NM] = fmaf(dv[e], T.vphi[p][(v4 + e) % NM], U[(v4 + e) / NM]);
             }
             float F[4], G[4];
             euler_flux_f(U, a.gamma, F, G);
@@ -324,8 +347,8 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
             if (a.stage == 1) {
                 o = un + dd;
             } else {
-                const double w = (double)sd[v * SD + slot] + dd;
-                sd[v * SD + slot] = (float)w;  // own slot: no other thread reads it any more
+                const double w = (double)sd[slot * VP + v] + dd;
+                sd[slot * VP + v] = (float)w;  // own slot: no other thread reads it any more
                 o = (a.stage == 2) ? 0.75 * un + 0.25 * w : (1.0 / 3.0) * un + (2.0 / 3.0) * w;
             }
             acc[q][m] = (float)o;
@@ -413,9 +436,9 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
         // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
         double e0 = 0.0;
         if (e_fix) {
-            const double rho0 = rho_clamp ? 1e-5 : (1.0 / 3.0) * a.un[k] + (2.0 / 3.0) * (double)sd[slot];
-            const double mx0 = (1.0 / 3.0) * a.un[(size_t)NM * plane + k] + (2.0 / 3.0) * (double)sd[NM * SD + slot];
-            const double my0 = (1.0 / 3.0) * a.un[(size_t)2 * NM * plane + k] + (2.0 / 3.0) * (double)sd[2 * NM * SD + slot];
+            const double rho0 = rho_clamp ? 1e-5 : (1.0 / 3.0) * a.un[k] + (2.0 / 3.0) * (double)sd[slot * VP];
+            const double mx0 = (1.0 / 3.0) * a.un[(size_t)NM * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + NM];
+            const double my0 = (1.0 / 3.0) * a.un[(size_t)2 * NM * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + 2 * NM];
             e0 = 1e-5 / (double)(a.gamma - 1.0f) + 0.5 * (mx0 * mx0 + my0 * my0) / rho0;
         }
 #pragma unroll
@@ -423,7 +446,7 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
 #pragma unroll
             for (int m = 0; m < NM; ++m) {
                 const int v = q * NM + m;
-                double o = (1.0 / 3.0) * a.un[(size_t)v * plane + k] + (2.0 / 3.0) * (double)sd[v * SD + slot];
+                double o = (1.0 / 3.0) * a.un[(size_t)v * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + v];
                 if (m == 0) {
                     if (q == 0 && rho_clamp) o = 1e-5;
                     if (q == 3 && e_fix) o = e0;
@@ -445,7 +468,7 @@ __global__ void __launch_bounds__(MNT, 2) dg_stage_mixed_kernel(MixArgs a) {
 template <int P>
 constexpr size_t smem_bytes() {
     constexpr int NQ = P + 1, NM = NQ * NQ;
-    return sizeof(float) * (4 * NM * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
+    return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
 }
 
 template <int P, typename TIn, typename TOut>
