@@ -175,18 +175,32 @@ __global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
                 ks = (size_t)a.gsrc[k];
                 neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
             }
-#pragma unroll 2
-            for (int v = 0; v < 4 * NM; v += 4) {
-                float4 x;
-                x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
-                x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
-                x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
-                x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
-                if (neg == (v + 0) / NM) x.x = -x.x;
-                if (neg == (v + 1) / NM) x.y = -x.y;
-                if (neg == (v + 2) / NM) x.z = -x.z;
-                if (neg == (v + 3) / NM) x.w = -x.w;
-                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
+            if (sizeof(TIn) == 4) {
+                // FP32 input: asynchronous 4-byte copies, all in flight at once
+                const float* src = static_cast<const float*>(a.cur) + ks;
+#pragma unroll 8
+                for (int v = 0; v < 4 * NM; ++v) {
+                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
+                                 : "memory");
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                if (neg >= 0)
+                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
+            } else {
+#pragma unroll 4
+                for (int v = 0; v < 4 * NM; v += 4) {
+                    float4 x;
+                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
+                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
+                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
+                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
+                    if (neg == (v + 0) / NM) x.x = -x.x;
+                    if (neg == (v + 1) / NM) x.y = -x.y;
+                    if (neg == (v + 2) / NM) x.z = -x.z;
+                    if (neg == (v + 3) / NM) x.w = -x.w;
+                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
+                }
             }
         } else {
             for (int v = 0; v < 4 * NM; v += 4)
@@ -277,7 +291,7 @@ __global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
         for (int m = 0; m < NM; ++m) acc[q][m] = 0.0f;
     if (kd == KIND_UPDATED) {
         const float* pc = sd + slot * VP;
-#pragma unroll
+#pragma unroll 4
         for (int p = 0; p < NV; ++p) {
             float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -336,23 +350,28 @@ __global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
     }
     // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
     const double dt = a.dt;
+    float* pw = sd + slot * VP;
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
+        float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
+        float cv[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            const int v = q * NM + m;
+        for (int e = 0; e < 4; ++e) {
+            const int v = v4 + e, q = v / NM, m = v % NM;
             const double un = a.un[(size_t)v * plane + k];
             const double dd = dt * (double)acc[q][m];
             double o;
             if (a.stage == 1) {
                 o = un + dd;
             } else {
-                const double w = (double)sd[slot * VP + v] + dd;
-                sd[slot * VP + v] = (float)w;  // own slot: no other thread reads it any more
+                const double w = (double)cv[e] + dd;
+                cv[e] = (float)w;
                 o = (a.stage == 2) ? 0.75 * un + 0.25 * w : (1.0 / 3.0) * un + (2.0 / 3.0) * w;
             }
             acc[q][m] = (float)o;
         }
+        if (a.stage != 1) *reinterpret_cast<float4*>(pw + v4) = make_float4(cv[0], cv[1], cv[2], cv[3]);  // own slot
+    }
 
     // limiter decisions in FP32 (src_DG/fluid.cpp:824-992), as factors
     float pf[4] = {1.0f, 1.0f, 1.0f, 1.0f};

@@ -58,38 +58,6 @@ __device__ __forceinline__ void weno5(T UL2, T UL1, T UP, T UR1, T UR2, T UR3, T
     UR = (e0 * qR0 + e1 * qR1 + e2 * qR2) / (e0 + e1 + e2);
 }
 
-// FP32 specialisation: the same weights w_k = (d_k / t_k^2) / sum_j (d_j / t_j^2)
-// with two reciprocals per side instead of four divisions.  With q_k = t_k^2
-// scaled by 1/max(q), w_k is proportional to d_k * prod_{j != k} q_j, every
-// factor in (0, 1]: no overflow; an underflow to 0 only drops a stencil whose
-// weight is negligible against the smoothest one, which keeps a factor of 1.
-template <>
-__device__ __forceinline__ void weno5<float>(float UL2, float UL1, float UP, float UR1, float UR2, float UR3,
-                                             float& UL, float& UR) {
-    const float eps = 1e-6f, C1 = 13.0f / 12.0f, C2 = 0.25f;
-    const float c13 = 1.0f / 3.0f, c76 = 7.0f / 6.0f, c116 = 11.0f / 6.0f, c16 = 1.0f / 6.0f, c56 = 5.0f / 6.0f;
-    auto combine = [&](float t0, float t1, float t2, float q0, float q1, float q2) {
-        float s0 = t0 * t0, s1 = t1 * t1, s2 = t2 * t2;
-        const float inv_m = 1.0f / fmaxf(s0, fmaxf(s1, s2));
-        s0 *= inv_m; s1 *= inv_m; s2 *= inv_m;
-        const float a0 = 0.1f * s1 * s2, a1 = 0.6f * s0 * s2, a2 = 0.3f * s0 * s1;
-        return (a0 * q0 + a1 * q1 + a2 * q2) / (a0 + a1 + a2);
-    };
-    const float qL0 = c13 * UL2 - c76 * UL1 + c116 * UP;
-    const float qL1 = -c16 * UL1 + c56 * UP + c13 * UR1;
-    const float qL2 = c13 * UP + c56 * UR1 - c16 * UR2;
-    const float d0 = UL2 - 2.0f * UL1 + UP, d1 = UL2 - 4.0f * UL1 + 3.0f * UP;
-    const float d2 = UL1 - 2.0f * UP + UR1, d3 = UL1 - UR1;
-    const float d4 = UP - 2.0f * UR1 + UR2, d5 = 3.0f * UP - 4.0f * UR1 + UR2;
-    const float b1 = eps + (C1 * d2 * d2 + C2 * d3 * d3);
-    UL = combine(eps + (C1 * d0 * d0 + C2 * d1 * d1), b1, eps + (C1 * d4 * d4 + C2 * d5 * d5), qL0, qL1, qL2);
-    const float qR0 = c116 * UR1 - c76 * UR2 + c13 * UR3;
-    const float r0 = UR1 - 2.0f * UR2 + UR3, r1 = 3.0f * UR1 - 4.0f * UR2 + UR3;
-    const float r3 = UP - UR2, r5 = UL1 - 4.0f * UP + 3.0f * UR1;
-    UR = combine(eps + (C1 * r0 * r0 + C2 * r1 * r1), eps + (C1 * d4 * d4 + C2 * r3 * r3),
-                 eps + (C1 * d2 * d2 + C2 * r5 * r5), qR0, qL2, qL1);
-}
-
 // std::min / std::max argument order of the reference, for either precision.
 template <typename T>
 __device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
