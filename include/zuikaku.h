@@ -131,6 +131,32 @@ int zk_step_timed(zk_ctx* ctx, double dt, int nsteps, float* ms);
  * doubles) and its row pitch in elements, for zero-copy callers. */
 int zk_state_device(zk_ctx* ctx, double** dptr, int* pitch);
 
+/* ---- learned troubled-cell indicator (no counterpart in the reference) ----
+ * A 40 -> 32 -> 32 -> 32 -> 1 GELU MLP gates the TVB limiter of
+ * ZK_LIMITER_TVB_MLP contexts: only cells with a positive logit take the
+ * characteristic-limiting branch.  Parameters are the flat FP32 block
+ * w1[32][40], b1[32], w2[32][32], b2[32], w3[32][32], b3[32], w4[32], b4
+ * (ZK_MLP_NPARAM floats), rounded to BF16 for inference. */
+#define ZK_MLP_NPARAM 3425
+#define ZK_MLP_IN 40
+int zk_set_indicator(zk_ctx* ctx, const float* params, int nparams);
+/* Per cell of the current (FP64) state: the indicator's 40 input features
+ * (features[ny*nx][40], may be NULL) and the plain TVB troubled-cell flag
+ * (labels[ny][nx], may be NULL).  The state is not modified. */
+int zk_indicator_features(zk_ctx* ctx, float* features, uint8_t* labels);
+/* Cells the TVB passes limited during the last zk_step (summed over stages). */
+int zk_limited_cells(zk_ctx* ctx, uint32_t* count);
+/* Training on the GPU (hand-written FP32 forward/backward + Adam kernels):
+ * X[n][40] features, y[n] labels (0/1); params in = initial, out = trained;
+ * batch a multiple of 64; loss = BCE on the logit with positive weight. */
+int zk_mlp_train(int device, const float* X, const uint8_t* y, int64_t n, float* params, int epochs, int batch,
+                 float lr, float pos_weight, uint64_t seed, float* epoch_loss);
+/* Mean loss and mean parameter gradient over n samples (gradient checks). */
+int zk_mlp_grad(int device, const float* X, const uint8_t* y, int64_t n, const float* params, float pos_weight,
+                float* grad, float* loss);
+/* Logits of n samples (bf16 != 0: BF16-rounded weights, as in inference). */
+int zk_mlp_forward(int device, const float* X, int64_t n, const float* params, int bf16, float* logits);
+
 /* FMA-throughput microbenchmark of one device: kind 0 = FP64, 1 = FP32;
  * writes the achieved dense TFLOP/s (2 flops per FMA).  Roofline denominator
  * for kernels bound by the FP pipes. */

@@ -480,3 +480,171 @@ void od_init_modes(int P, int ny, int nx, const double* U, double* dof) {
     memset(dof, 0, sizeof(double) * 4 * NM * plane);
     for (int c = 0; c < 4; ++c) memcpy(&DOF(dof, c, 0, 0), U + c * plane, sizeof(double) * plane);
 }
+
+/* ---- TVB limiter (no reference implementation) ------------------------------
+ * Cockburn & Shu (2001, J. Sci. Comput. 16; cited in the reference README) TVB
+ * minmod limiting of the linear modes with characteristic decomposition, in
+ * the form the reference's own header documents for its DG limiter
+ * (src_DG/fluid.h:140-147: minmod on u_{1,0}, u_{0,1}; if limited, the modes
+ * with px+py > 1 are set to zero).  Per bctype-0 cell in the update range:
+ *   slopes  a_x = mode (1,0), a_y = mode (0,1); mean differences to the
+ *           neighbours (filled through the ghost map) D+ and D-;
+ *   in characteristic variables of the mean state (x or y eigenvectors),
+ *   w~ = m~(w, w+, w-) with m~(a,b,c) = a if |a| <= M h^2 else minmod(a,b,c);
+ *   a cell is troubled when any w~ differs from w; a troubled cell gets the
+ *   limited linear modes (R w~) and zero higher modes.
+ * Cell means are never modified, so the pass reads neighbour means from the
+ * same array it writes (a Jacobi sweep). */
+
+/* Left (L) and right (R) eigenvectors of the Euler flux Jacobian in direction
+ * dir (0 = x, 1 = y) at conserved state u; returns 0 for a non-physical state. */
+int od_euler_eigen(const double u[4], double gamma, int dir, double L[4][4], double R[4][4]) {
+    const double rho = u[0];
+    if (!(rho > 0.0)) return 0;
+    const double vx = u[1] / rho, vy = u[2] / rho;
+    const double q2 = vx * vx + vy * vy;
+    const double p = (gamma - 1.0) * (u[3] - 0.5 * rho * q2);
+    if (!(p > 0.0)) return 0;
+    const double c = sqrt(gamma * p / rho);
+    const double H = (u[3] + p) / rho;
+    const double b1 = (gamma - 1.0) / (c * c), b2 = 0.5 * q2 * b1;
+    const double un = dir == 0 ? vx : vy;   /* normal velocity */
+    const double ut = dir == 0 ? vy : vx;   /* tangential velocity */
+    const int in = dir == 0 ? 1 : 2, it = dir == 0 ? 2 : 1;  /* momentum slots */
+    for (int r = 0; r < 4; ++r)
+        for (int k = 0; k < 4; ++k) L[r][k] = R[r][k] = 0.0;
+    /* right eigenvectors as columns: (un-c), (un) entropy, (un) shear, (un+c) */
+    R[0][0] = 1.0; R[in][0] = un - c; R[it][0] = ut; R[3][0] = H - un * c;
+    R[0][1] = 1.0; R[in][1] = un;     R[it][1] = ut; R[3][1] = 0.5 * q2;
+    R[0][2] = 0.0; R[in][2] = 0.0;    R[it][2] = 1.0; R[3][2] = ut;
+    R[0][3] = 1.0; R[in][3] = un + c; R[it][3] = ut; R[3][3] = H + un * c;
+    /* left eigenvectors as rows (L = R^-1) */
+    L[0][0] = 0.5 * (b2 + un / c); L[0][in] = -0.5 * (b1 * un + 1.0 / c); L[0][it] = -0.5 * b1 * ut; L[0][3] = 0.5 * b1;
+    L[1][0] = 1.0 - b2;            L[1][in] = b1 * un;                    L[1][it] = b1 * ut;         L[1][3] = -b1;
+    L[2][0] = -ut;                 L[2][in] = 0.0;                        L[2][it] = 1.0;             L[2][3] = 0.0;
+    L[3][0] = 0.5 * (b2 - un / c); L[3][in] = -0.5 * (b1 * un - 1.0 / c); L[3][it] = -0.5 * b1 * ut; L[3][3] = 0.5 * b1;
+    return 1;
+}
+
+static double tvb_minmod(double a, double b, double c, double mh2) {
+    if (fabs(a) <= mh2) return a;
+    if (a > 0.0 && b > 0.0 && c > 0.0) return zk_min(a, zk_min(b, c));
+    if (a < 0.0 && b < 0.0 && c < 0.0) return zk_max(a, zk_max(b, c));
+    return 0.0;
+}
+
+/* Limit one direction: slope a[4] against D+ dp[4] and D- dm[4] at mean ub.
+ * Returns 1 (troubled) and writes the limited slope, else 0. */
+static int tvb_dir(const double ub[4], double gamma, int dir, double mh2, const double a[4],
+                   const double dp[4], const double dm[4], double out[4]) {
+    double L[4][4], R[4][4];
+    const int phys = od_euler_eigen(ub, gamma, dir, L, R);
+    double w[4], wp[4], wm[4], wl[4];
+    for (int r = 0; r < 4; ++r) {
+        if (phys) {
+            w[r] = L[r][0] * a[0] + L[r][1] * a[1] + L[r][2] * a[2] + L[r][3] * a[3];
+            wp[r] = L[r][0] * dp[0] + L[r][1] * dp[1] + L[r][2] * dp[2] + L[r][3] * dp[3];
+            wm[r] = L[r][0] * dm[0] + L[r][1] * dm[1] + L[r][2] * dm[2] + L[r][3] * dm[3];
+        } else {
+            w[r] = a[r]; wp[r] = dp[r]; wm[r] = dm[r];   /* component-wise fallback */
+        }
+    }
+    int changed = 0;
+    for (int r = 0; r < 4; ++r) {
+        wl[r] = tvb_minmod(w[r], wp[r], wm[r], mh2);
+        if (wl[r] != w[r]) changed = 1;
+    }
+    if (!changed) return 0;
+    for (int r = 0; r < 4; ++r)
+        out[r] = phys ? R[r][0] * wl[0] + R[r][1] * wl[1] + R[r][2] * wl[2] + R[r][3] * wl[3] : wl[r];
+    return 1;
+}
+
+/* Mean (mode 0) of cell k's neighbour, gathered through the fill map. */
+static void nb_mean(const od_ctx* x, const double* d, size_t k, double out[4]) {
+    const int NM = x->NM;
+    const size_t plane = x->plane;
+    size_t s = k;
+    int neg = -1;
+    if (x->src[k] >= 0) {
+        s = (size_t)x->src[k];
+        neg = x->kind[k] == ZK_CELL_SLIP_X ? 1 : (x->kind[k] == ZK_CELL_SLIP_Y ? 2 : -1);
+    }
+    for (int c = 0; c < 4; ++c) {
+        const double v = DOF(d, c, 0, s);
+        out[c] = (neg == c) ? -v : v;
+    }
+}
+
+static void limit_tvb_all(const od_ctx* x, double da, double gamma, double M, double* d, unsigned char* flags) {
+    const int P = x->P, NM = x->NM, nx = x->nx;
+    const size_t plane = x->plane;
+    const double mh2 = M * da * da;
+    const int mx = P + 1, my = 1;  /* modes (px,py) = (1,0) and (0,1) */
+    for (size_t k = 0; k < plane; ++k) {
+        if (flags) flags[k] = 0;
+        if (x->kind[k] != ZK_CELL_UPDATED) continue;
+        double ub[4], uL[4], uR[4], uU[4], uD[4];
+        for (int c = 0; c < 4; ++c) ub[c] = DOF(d, c, 0, k);
+        nb_mean(x, d, k - 1, uL);
+        nb_mean(x, d, k + 1, uR);
+        nb_mean(x, d, k - (size_t)nx, uU);
+        nb_mean(x, d, k + (size_t)nx, uD);
+        double ax[4], ay[4], dxp[4], dxm[4], dyp[4], dym[4], lx[4], ly[4];
+        for (int c = 0; c < 4; ++c) {
+            ax[c] = DOF(d, c, mx, k);
+            ay[c] = DOF(d, c, my, k);
+            dxp[c] = uR[c] - ub[c];
+            dxm[c] = ub[c] - uL[c];
+            dyp[c] = uD[c] - ub[c];  /* eta grows with the row index */
+            dym[c] = ub[c] - uU[c];
+        }
+        const int tx = tvb_dir(ub, gamma, 0, mh2, ax, dxp, dxm, lx);
+        const int ty = tvb_dir(ub, gamma, 1, mh2, ay, dyp, dym, ly);
+        if (!(tx || ty)) continue;
+        if (flags) flags[k] = 1;
+        for (int c = 0; c < 4; ++c) {
+            if (tx) DOF(d, c, mx, k) = lx[c];
+            if (ty) DOF(d, c, my, k) = ly[c];
+            for (int m = 0; m < NM; ++m)
+                if (m / (P + 1) + m % (P + 1) > 1) DOF(d, c, m, k) = 0.0;
+        }
+    }
+}
+
+/* One TVB pass on the state (ghost map built from bct; periodic ring -3). */
+int od_limit_tvb(int P, int ny, int nx, double da, double gamma, double* dof, const int* bct, double M,
+                 int periodic, unsigned char* flags) {
+    if (P < 1 || P > 3) return 1;
+    od_ctx x = ctx_new(P, ny, nx, bct, periodic);
+    limit_tvb_all(&x, da, gamma, M, dof, flags);
+    ctx_free(&x);
+    return 0;
+}
+
+/* updateMesh with a selectable limiter after each stage:
+ * 0 = reference (Persson + Zhang-Shu), 1 = none, 2 = TVB(M). */
+int od_step_lim(int P, int ny, int nx, double da, double gamma, double* dof, const int* bct, double dt,
+                int nsteps, int periodic, int hll, int limiter, double M) {
+    if (P < 1 || P > 3) return 1;
+    od_ctx x = ctx_new(P, ny, nx, bct, periodic);
+    const size_t n = (size_t)4 * x.NM * x.plane;
+    double* dn = (double*)malloc(sizeof(double) * n);
+    double* dU = (double*)malloc(sizeof(double) * n);
+    for (int s = 0; s < nsteps; ++s) {
+        memcpy(dn, dof, sizeof(double) * n);
+        for (int stage = 1; stage <= 3; ++stage) {
+            rhs_all(&x, da, gamma, dof, hll, dU);
+            for (size_t k = 0; k < n; ++k) {
+                if (stage == 1) dof[k] = dn[k] + dt * dU[k];
+                else if (stage == 2) dof[k] = 0.75 * dn[k] + 0.25 * (dof[k] + dt * dU[k]);
+                else dof[k] = (1.0 / 3.0) * dn[k] + (2.0 / 3.0) * (dof[k] + dt * dU[k]);
+            }
+            if (limiter == 0) limit_all(&x, bct, gamma, dof);
+            else if (limiter == 2) limit_tvb_all(&x, da, gamma, M, dof, NULL);
+        }
+    }
+    free(dn); free(dU);
+    ctx_free(&x);
+    return 0;
+}

@@ -79,6 +79,11 @@ class Restatement:
         L.od_hlle.argtypes = [_D, _D, C.c_double, _D]
         L.od_phi2.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
         L.od_phi2.restype = C.c_double
+        L.od_euler_eigen.argtypes = [_D, C.c_double, C.c_int, _D, _D]
+        L.od_limit_tvb.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double,
+                                   C.c_int, C.POINTER(C.c_uint8)]
+        L.od_step_lim.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double,
+                                  C.c_int, C.c_int, C.c_int, C.c_int, C.c_double]
         self.L = L
 
     # WENO -----------------------------------------------------------------------
@@ -147,6 +152,30 @@ class Restatement:
         b = np.ascontiguousarray(bct, dtype=np.int32)
         rc = self.L.od_step(P, b.shape[0], b.shape[1], da, gamma, _d(d), _i(b), dt, int(nsteps),
                             int(periodic), int(hll))
+        assert rc == 0
+        return d
+
+    def euler_eigen(self, u, gamma, direction):
+        u = np.ascontiguousarray(u, np.float64)
+        L = np.zeros((4, 4)); R = np.zeros((4, 4))
+        ok = self.L.od_euler_eigen(_d(u), gamma, direction, _d(L), _d(R))
+        return bool(ok), L, R
+
+    def dg_limit_tvb(self, P, dof, bct, da, gamma, M=50.0, periodic=False):
+        """One TVB pass; returns (limited dof, troubled-cell flags)."""
+        d = np.array(dof, dtype=np.float64, order="C")
+        b = np.ascontiguousarray(bct, dtype=np.int32)
+        fl = np.zeros(b.shape, np.uint8)
+        self.L.od_limit_tvb(P, b.shape[0], b.shape[1], da, gamma, _d(d), _i(b), M, int(periodic),
+                            fl.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return d, fl
+
+    def dg_step_lim(self, P, dof, bct, da, gamma, dt, nsteps=1, limiter="tvb", M=50.0, periodic=False, hll=False):
+        code = {"reference": 0, "none": 1, "tvb": 2}[limiter]
+        d = np.array(dof, dtype=np.float64, order="C")
+        b = np.ascontiguousarray(bct, dtype=np.int32)
+        rc = self.L.od_step_lim(P, b.shape[0], b.shape[1], da, gamma, _d(d), _i(b), dt, int(nsteps),
+                                int(periodic), int(hll), code, M)
         assert rc == 0
         return d
 

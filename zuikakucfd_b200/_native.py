@@ -20,6 +20,8 @@ PRECISION = {"fp64": 0, "mixed": 1}
 LIMITER = {"reference": 0, "none": 1, "tvb": 2, "tvb_mlp": 3}
 FLUX = {"hllc": 0, "hll": 1}
 BOUNDARY = {"exchange": 0, "periodic": 1}
+MLP_NPARAM = 3425
+MLP_IN = 40
 
 
 class ZkError(RuntimeError):
@@ -63,6 +65,16 @@ _SIGS = {
     "zk_step_timed": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(C.c_float)]),
     "zk_state_device": (C.c_int, [_P, C.POINTER(_D), C.POINTER(C.c_int)]),
     "zk_peak_flops": (C.c_int, [C.c_int, C.c_int, _D]),
+    "zk_set_indicator": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int]),
+    "zk_indicator_features": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
+    "zk_limited_cells": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "zk_mlp_train": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.c_int64,
+                               C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64,
+                               C.POINTER(C.c_float)]),
+    "zk_mlp_grad": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.c_int64,
+                              C.POINTER(C.c_float), C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "zk_mlp_forward": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.c_int64, C.POINTER(C.c_float), C.c_int,
+                                 C.POINTER(C.c_float)]),
     "zk_weno_step_noalloc": (C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int32), C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_uint32)]),

@@ -39,6 +39,8 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("dg_fp64.cu", STRICT),
     ("dg_driver.cu", []),
     ("dg_mixed.cu", ["--use_fast_math"]),
+    ("dg_tvb.cu", STRICT),
+    ("mlp.cu", []),
     ("peak.cu", []),
     ("weno_mixed.cu", ["--use_fast_math"]),
     ("noalloc.cu", []),

@@ -2,13 +2,21 @@
 // (src_DG/fluid.cpp:1005-1054) on the device state.
 #include <cmath>
 
+#include <vector>
+
+#include <cuda_bf16.h>
+
 #include "dg_common.cuh"
 #include "zk_internal.h"
+#include "zk_mlp.h"
 
 namespace zk {
 cudaError_t launch_dg_stage_fp64(int P, const DGArgs& a, cudaStream_t s);
 cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s);
 int dg_upload_tables_f32(int P);
+cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
+                          double da, double gamma, double M, uint8_t* flags, const MlpWeights* mlp,
+                          float* features, uint32_t* nflag, cudaStream_t s);
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
@@ -54,8 +62,8 @@ int cuda_fail(cudaError_t e) { return zk_internal_fail(ZK_ERR_CUDA, cudaGetError
 
 int zk_dg_setup(zk_ctx* c) {
     const int P = c->opt.order;
-    if (c->opt.limiter != ZK_LIMITER_REFERENCE && c->opt.limiter != ZK_LIMITER_NONE)
-        return zk_internal_fail(ZK_ERR_UNSUPPORTED, "DG TVB limiters are not available in this build");
+    if (c->opt.limiter >= ZK_LIMITER_TVB && !(c->opt.tvb_M >= 0.0))
+        return zk_internal_fail(ZK_ERR_ARG, "TVB constant M must be >= 0");
     DGState* s = new DGState();
     c->dg = s;
     zk::DGTab tab;
@@ -78,7 +86,25 @@ int zk_dg_setup(zk_ctx* c) {
         if (e == cudaSuccess) e = cudaMemsetAsync(c->F1, 0, sizeof(float) * n, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->F2, 0, sizeof(float) * n, c->stream);
     }
+    if (e == cudaSuccess && !c->d_flags) e = cudaMalloc(&c->d_flags, c->g.plane);
+    if (e == cudaSuccess && !c->d_nflag) e = cudaMalloc(&c->d_nflag, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_nflag, 0, sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess && c->opt.limiter == ZK_LIMITER_TVB_MLP && !c->mlp)
+        e = cudaMalloc(&c->mlp, sizeof(zk::MlpWeights));
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
+// TVB pass (plain or indicator-gated) on a stage output, when configured.
+int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64) {
+    if (c->opt.limiter < ZK_LIMITER_TVB) return ZK_OK;
+    const zk::MlpWeights* w = nullptr;
+    if (c->opt.limiter == ZK_LIMITER_TVB_MLP) {
+        if (!c->mlp_set) return zk_internal_fail(ZK_ERR_STATE, "indicator weights not set (zk_set_indicator)");
+        w = static_cast<const zk::MlpWeights*>(c->mlp);
+    }
+    cudaError_t e = zk::launch_dg_tvb(c->opt.order, state, fp64, c->kind, c->gsrc, c->g, c->da, c->gamma,
+                                      c->opt.tvb_M, c->d_flags, w, nullptr, c->d_nflag, c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }
 
@@ -89,6 +115,12 @@ void zk_dg_release(zk_ctx* c) {
     if (s->fy) cudaFree(s->fy);
     delete s;
     c->dg = nullptr;
+    for (void* p : {(void*)c->mlp, (void*)c->d_flags, (void*)c->d_nflag})
+        if (p) cudaFree(p);
+    c->mlp = nullptr;
+    c->d_flags = nullptr;
+    c->d_nflag = nullptr;
+    c->mlp_set = false;
 }
 
 static int dg_step_mixed(zk_ctx* c, double dt) {
@@ -96,22 +128,30 @@ static int dg_step_mixed(zk_ctx* c, double dt) {
     const double s0 = st(c)->s0;
     cudaError_t e = zk::launch_dg_stage_mixed(P, c->Un, 1, c->Un, c->F1, 0, c->kind, c->gsrc, c->g, dt, c->da,
                                               c->gamma, 1, lim, hll, s0, c->d_status, c->stream);
-    if (e == cudaSuccess)
-        e = zk::launch_dg_stage_mixed(P, c->F1, 0, c->Un, c->F2, 0, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 2,
-                                      lim, hll, s0, c->d_status, c->stream);
-    if (e == cudaSuccess)
-        e = zk::launch_dg_stage_mixed(P, c->F2, 0, c->Un, c->Un, 1, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 3,
-                                      lim, hll, s0, c->d_status, c->stream);
-    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (int rc = zk_dg_after_stage(c, c->F1, false)) return rc;
+    e = zk::launch_dg_stage_mixed(P, c->F1, 0, c->Un, c->F2, 0, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 2,
+                                  lim, hll, s0, c->d_status, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (int rc = zk_dg_after_stage(c, c->F2, false)) return rc;
+    e = zk::launch_dg_stage_mixed(P, c->F2, 0, c->Un, c->Un, 1, c->kind, c->gsrc, c->g, dt, c->da, c->gamma, 3,
+                                  lim, hll, s0, c->d_status, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    return zk_dg_after_stage(c, c->Un, true);
 }
 
 int zk_dg_step(zk_ctx* c, double dt) {
     if (c->opt.precision == ZK_PREC_MIXED) return dg_step_mixed(c, dt);
     const int P = c->opt.order;
     cudaError_t e = zk::launch_dg_stage_fp64(P, args(c, c->Un, c->Un, c->S1, dt, 1), c->stream);
-    if (e == cudaSuccess) e = zk::launch_dg_stage_fp64(P, args(c, c->S1, c->Un, c->S2, dt, 2), c->stream);
-    if (e == cudaSuccess) e = zk::launch_dg_stage_fp64(P, args(c, c->S2, c->Un, c->Un, dt, 3), c->stream);
-    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (int rc = zk_dg_after_stage(c, c->S1, true)) return rc;
+    e = zk::launch_dg_stage_fp64(P, args(c, c->S1, c->Un, c->S2, dt, 2), c->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    if (int rc = zk_dg_after_stage(c, c->S2, true)) return rc;
+    e = zk::launch_dg_stage_fp64(P, args(c, c->S2, c->Un, c->Un, dt, 3), c->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    return zk_dg_after_stage(c, c->Un, true);
 }
 
 int zk_dg_rhs(zk_ctx* c, double* dU_dev) {
@@ -120,7 +160,50 @@ int zk_dg_rhs(zk_ctx* c, double* dU_dev) {
 }
 
 int zk_dg_limit(zk_ctx* c) {
+    if (c->opt.limiter >= ZK_LIMITER_TVB) return zk_dg_after_stage(c, c->Un, true);
     zk::DGArgs a = args(c, c->Un, c->Un, c->Un, 0.0, 1);
     cudaError_t e = zk::launch_dg_limit_fp64(c->opt.order, a, c->stream);
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
+// ---- learned indicator: weights, features, counters ------------------------------
+extern "C" int zk_set_indicator(zk_ctx* c, const float* params, int nparams) {
+    if (!c || !params) return zk_internal_fail(ZK_ERR_ARG, "null argument");
+    if (nparams != zk::MLP_NPARAM) return zk_internal_fail(ZK_ERR_ARG, "indicator needs exactly MLP_NPARAM parameters");
+    if (c->opt.limiter != ZK_LIMITER_TVB_MLP || !c->mlp)
+        return zk_internal_fail(ZK_ERR_STATE, "context is not a DG TVB_MLP context with a mesh");
+    std::vector<float> w(params, params + nparams);
+    for (float& x : w) x = __bfloat162float(__float2bfloat16(x));  // BF16 inference weights
+    cudaError_t e = cudaMemcpyAsync(c->mlp, w.data(), sizeof(float) * nparams, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(e);
+    c->mlp_set = true;
+    return ZK_OK;
+}
+
+extern "C" int zk_indicator_features(zk_ctx* c, float* features, uint8_t* labels) {
+    if (!c || !c->Un || c->opt.method != ZK_METHOD_DG) return zk_internal_fail(ZK_ERR_STATE, "needs a DG context with a mesh");
+    const size_t ncell = (size_t)c->g.ny * c->g.nx;
+    float* df = nullptr;
+    cudaError_t e = cudaMalloc(&df, sizeof(float) * zk::MLP_IN * ncell);
+    if (e == cudaSuccess) e = cudaMemsetAsync(df, 0, sizeof(float) * zk::MLP_IN * ncell, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_dg_tvb(c->opt.order, c->Un, true, c->kind, c->gsrc, c->g, c->da, c->gamma, c->opt.tvb_M,
+                              c->d_flags, nullptr, df, nullptr, c->stream);
+    if (e == cudaSuccess && features)
+        e = cudaMemcpyAsync(features, df, sizeof(float) * zk::MLP_IN * ncell, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && labels)
+        e = cudaMemcpy2DAsync(labels, c->g.nx, c->d_flags, c->g.pitch, c->g.nx, c->g.ny, cudaMemcpyDeviceToHost,
+                              c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (df) cudaFree(df);
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
+extern "C" int zk_limited_cells(zk_ctx* c, uint32_t* count) {
+    if (!c || !count) return zk_internal_fail(ZK_ERR_ARG, "null argument");
+    if (!c->d_nflag) { *count = 0; return ZK_OK; }
+    cudaError_t e = cudaMemcpyAsync(count, c->d_nflag, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }

@@ -352,6 +352,7 @@ int zk_step(zk_ctx* c, double dt, int nsteps) {
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(ZK_ERR_ARG, "dt must be finite and > 0");
     ZK_CUDA(cudaSetDevice(c->opt.device));
     ZK_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), c->stream));
+    if (c->d_nflag) ZK_CUDA(cudaMemsetAsync(c->d_nflag, 0, sizeof(uint32_t), c->stream));
     if (int rc = enqueue_steps(c, dt, nsteps)) return rc;
     ZK_CUDA(cudaStreamSynchronize(c->stream));
     return ZK_OK;

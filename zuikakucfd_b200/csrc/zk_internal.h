@@ -36,6 +36,10 @@ struct zk_ctx {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void* dg = nullptr;  // DG driver state
+    void* mlp = nullptr;          // device MlpWeights (learned indicator), BF16-rounded
+    bool mlp_set = false;
+    uint8_t* d_flags = nullptr;   // TVB troubled-cell flags of the last pass, pitched
+    uint32_t* d_nflag = nullptr;  // cells the TVB passes limited during the last zk_step
 };
 
 int zk_internal_fail(int code, const char* msg);
@@ -46,6 +50,7 @@ void zk_dg_release(zk_ctx* c);
 int zk_dg_step(zk_ctx* c, double dt);
 int zk_dg_rhs(zk_ctx* c, double* dU_dev);
 int zk_dg_limit(zk_ctx* c);
+int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64);
 
 // WENO mixed-precision driver (weno_mixed.cu)
 int zk_weno_mixed_setup(zk_ctx* c);

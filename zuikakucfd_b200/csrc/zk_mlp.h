@@ -1,0 +1,62 @@
+// The learned troubled-cell indicator: a 40 -> 32 -> 32 -> 32 -> 1 MLP with
+// GELU activations.  Inputs (per cell, from the FP64/FP32 DG state):
+//   f[0..15]   rho modes, slot px*4+py, divided by s_rho = max |rho mean| over
+//              the cell and its 4 neighbours
+//   f[16..31]  E modes, same slots, divided by s_E
+//   f[32..35]  (rho mean of neighbour L, R, U, D - own rho mean) / s_rho
+//   f[36..39]  the same for E
+// Output: a logit; > 0 flags the cell for TVB characteristic limiting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace zk {
+
+constexpr int MLP_IN = 40, MLP_H = 32;
+constexpr int MLP_NPARAM = MLP_H * MLP_IN + MLP_H + 2 * (MLP_H * MLP_H + MLP_H) + MLP_H + 1;
+
+// Parameters in one flat block (row-major weights, out x in).  For inference
+// the values are BF16-rounded copies of the FP32 trained parameters.
+struct MlpWeights {
+    float w1[MLP_H][MLP_IN];
+    float b1[MLP_H];
+    float w2[MLP_H][MLP_H];
+    float b2[MLP_H];
+    float w3[MLP_H][MLP_H];
+    float b3[MLP_H];
+    float w4[MLP_H];
+    float b4;
+};
+static_assert(sizeof(MlpWeights) == sizeof(float) * MLP_NPARAM, "MlpWeights must be a flat float block");
+
+__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+
+// Plain FP32 forward pass (CUDA cores).
+__device__ __forceinline__ float mlp_logit(const MlpWeights& W, const float f[MLP_IN]) {
+    float h1[MLP_H], h2[MLP_H];
+#pragma unroll 4
+    for (int o = 0; o < MLP_H; ++o) {
+        float s = W.b1[o];
+#pragma unroll
+        for (int i = 0; i < MLP_IN; ++i) s = fmaf(W.w1[o][i], f[i], s);
+        h1[o] = gelu(s);
+    }
+#pragma unroll 4
+    for (int o = 0; o < MLP_H; ++o) {
+        float s = W.b2[o];
+#pragma unroll
+        for (int i = 0; i < MLP_H; ++i) s = fmaf(W.w2[o][i], h1[i], s);
+        h2[o] = gelu(s);
+    }
+    float out = W.b4;
+#pragma unroll 4
+    for (int o = 0; o < MLP_H; ++o) {
+        float s = W.b3[o];
+#pragma unroll
+        for (int i = 0; i < MLP_H; ++i) s = fmaf(W.w3[o][i], h2[i], s);
+        out = fmaf(W.w4[o], gelu(s), out);
+    }
+    return out;
+}
+
+}  // namespace zk
