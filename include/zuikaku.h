@@ -137,7 +137,7 @@ int zk_state_device(zk_ctx* ctx, double** dptr, int* pitch);
  * characteristic-limiting branch.  Parameters are the flat FP32 block
  * w1[32][40], b1[32], w2[32][32], b2[32], w3[32][32], b3[32], w4[32], b4
  * (ZK_MLP_NPARAM floats), rounded to BF16 for inference. */
-#define ZK_MLP_NPARAM 3425
+#define ZK_MLP_NPARAM 3457
 #define ZK_MLP_IN 40
 int zk_set_indicator(zk_ctx* ctx, const float* params, int nparams);
 /* Per cell of the current (FP64) state: the indicator's 40 input features

@@ -26,4 +26,4 @@ def test_oracle_gradient_matches_finite_differences():
 
 def test_param_count_matches_abi():
     from zuikakucfd_b200 import _native
-    assert M.NPARAM == _native.MLP_NPARAM == 3425
+    assert M.NPARAM == _native.MLP_NPARAM == 3457

@@ -20,7 +20,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 LIMITER = {"reference": 0, "none": 1, "tvb": 2, "tvb_mlp": 3}
 FLUX = {"hllc": 0, "hll": 1}
 BOUNDARY = {"exchange": 0, "periodic": 1}
-MLP_NPARAM = 3425
+MLP_NPARAM = 3457
 MLP_IN = 40
 
 
