@@ -144,6 +144,9 @@ int zk_set_indicator(zk_ctx* ctx, const float* params, int nparams);
  * (features[ny*nx][40], may be NULL) and the plain TVB troubled-cell flag
  * (labels[ny][nx], may be NULL).  The state is not modified. */
 int zk_indicator_features(zk_ctx* ctx, float* features, uint8_t* labels);
+/* The indicator's logits[ny*nx] for the current state, computed by the
+ * tensor-core inference path the limiter uses (0 for non-updated cells). */
+int zk_indicator_logits(zk_ctx* ctx, float* logits);
 /* Cells the TVB passes limited during the last zk_step (summed over stages). */
 int zk_limited_cells(zk_ctx* ctx, uint32_t* count);
 /* Training on the GPU (hand-written FP32 forward/backward + Adam kernels):

@@ -108,3 +108,72 @@ def test_training_learns_a_separable_rule():
     assert losses[-1] < 0.5 * losses[0]
     ag = indicator.agreement(p, X, y)
     assert ag["accuracy"] > 0.97 and ag["missed_rate"] < 0.1
+
+
+def test_shipped_indicator_gates_tvb_limiting():
+    """The trained indicator (zuikakucfd_b200/data/indicator_p3.npz) on a
+    held-out seed: the gated run limits cells close to where plain TVB does,
+    stays finite and positive, and its solution is close to the plain-TVB
+    run; an unlimited run of the same case is the contrast."""
+    from zuikakucfd_b200 import _native as N, cases, indicator
+    P = 3
+    c = cases.four_quadrant(256, seed=9100)
+    lam = c.da / cases.cfl_dt(c, 1.0)
+    dt = 0.5 * 0.9 / (2 * (2 * P + 1)) * c.da / lam
+    w = indicator.load()
+    runs, counts = {}, {}
+    for lim in ("tvb", "tvb_mlp", "none"):
+        with dg_solver(P, c, lim, precision="mixed") as s:
+            if lim == "tvb_mlp":
+                N.check(N.lib().zk_set_indicator(s._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
+            s.set_state(c.dg_state(P))
+            total = 0
+            for _ in range(10):
+                s.step(dt, 6)
+                n = C.c_uint32()
+                N.check(N.lib().zk_limited_cells(s._h, C.byref(n)))
+                total += n.value
+            runs[lim] = (s.get_state(), s.status_word())
+            counts[lim] = total
+    tvb, st_t = runs["tvb"]
+    mlp, st_m = runs["tvb_mlp"]
+    assert st_t == 0 and st_m == 0
+    assert np.isfinite(mlp).all() and mlp[0, 0, 3:-3, 3:-3].min() > 0
+    assert counts["tvb_mlp"] > 0.5 * counts["tvb"]
+    d = np.abs(mlp[0, 0] - tvb[0, 0]).sum() / np.abs(tvb[0, 0]).sum()
+    assert d < 5e-3, d
+
+
+def test_indicator_requires_weights():
+    from zuikakucfd_b200 import cases
+    from zuikakucfd_b200._native import ZkError
+    c = cases.four_quadrant(32, seed=1)
+    with dg_solver(3, c, "tvb_mlp") as s:
+        s.set_state(c.dg_state(3))
+        with pytest.raises(ZkError, match="indicator weights not set"):
+            s.step(1e-4, 1)
+
+
+def test_tensor_core_inference_matches_fp32_forward():
+    """The limiter's BF16 mma.sync inference against the FP32 forward pass on
+    the same features: logits close, decisions agree."""
+    from zuikakucfd_b200 import _native as N, cases, indicator
+    P = 3
+    c = cases.four_quadrant(96, seed=9200)
+    lam = c.da / cases.cfl_dt(c, 1.0)
+    dt = 0.5 * 0.9 / (2 * (2 * P + 1)) * c.da / lam
+    w = indicator.load()
+    with dg_solver(P, c, "tvb_mlp") as s:
+        N.check(N.lib().zk_set_indicator(s._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
+        s.set_state(c.dg_state(P))
+        s.step(dt, 8)
+        X, y = indicator.features_and_labels(s)
+        z = np.zeros(c.ny * c.nx, np.float32)
+        N.check(N.lib().zk_indicator_logits(s._h, z.ctypes.data_as(C.POINTER(C.c_float))))
+    upd = np.zeros((c.ny, c.nx), bool)
+    upd[3:-3, 3:-3] = True
+    upd = upd.ravel()
+    zr = indicator.logits(w, X[upd], bf16=True)
+    zt = z[upd]
+    assert np.abs(zt - zr).max() <= 0.05 * max(1.0, np.abs(zr).max())
+    assert ((zt > 0) == (zr > 0)).mean() >= 0.995

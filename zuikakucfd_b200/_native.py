@@ -68,6 +68,7 @@ _SIGS = {
     "zk_set_indicator": (C.c_int, [_P, C.POINTER(C.c_float), C.c_int]),
     "zk_indicator_features": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
     "zk_limited_cells": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "zk_indicator_logits": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "zk_mlp_train": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.c_int64,
                                C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64,
                                C.POINTER(C.c_float)]),

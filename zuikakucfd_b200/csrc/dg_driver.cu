@@ -16,7 +16,7 @@ cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s);
 int dg_upload_tables_f32(int P);
 cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
                           double da, double gamma, double M, uint8_t* flags, const MlpWeights* mlp,
-                          float* features, uint32_t* nflag, cudaStream_t s);
+                          float* features, uint32_t* nflag, float* logits, cudaStream_t s);
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
@@ -104,7 +104,7 @@ int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64) {
         w = static_cast<const zk::MlpWeights*>(c->mlp);
     }
     cudaError_t e = zk::launch_dg_tvb(c->opt.order, state, fp64, c->kind, c->gsrc, c->g, c->da, c->gamma,
-                                      c->opt.tvb_M, c->d_flags, w, nullptr, c->d_nflag, c->stream);
+                                      c->opt.tvb_M, c->d_flags, w, nullptr, c->d_nflag, nullptr, c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }
 
@@ -189,7 +189,7 @@ extern "C" int zk_indicator_features(zk_ctx* c, float* features, uint8_t* labels
     if (e == cudaSuccess) e = cudaMemsetAsync(df, 0, sizeof(float) * zk::MLP_IN * ncell, c->stream);
     if (e == cudaSuccess)
         e = zk::launch_dg_tvb(c->opt.order, c->Un, true, c->kind, c->gsrc, c->g, c->da, c->gamma, c->opt.tvb_M,
-                              c->d_flags, nullptr, df, nullptr, c->stream);
+                              c->d_flags, nullptr, df, nullptr, nullptr, c->stream);
     if (e == cudaSuccess && features)
         e = cudaMemcpyAsync(features, df, sizeof(float) * zk::MLP_IN * ncell, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && labels)
@@ -205,5 +205,22 @@ extern "C" int zk_limited_cells(zk_ctx* c, uint32_t* count) {
     if (!c->d_nflag) { *count = 0; return ZK_OK; }
     cudaError_t e = cudaMemcpyAsync(count, c->d_nflag, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
+extern "C" int zk_indicator_logits(zk_ctx* c, float* logits) {
+    if (!c || !logits) return zk_internal_fail(ZK_ERR_ARG, "null argument");
+    if (!c->Un || c->opt.limiter != ZK_LIMITER_TVB_MLP || !c->mlp_set)
+        return zk_internal_fail(ZK_ERR_STATE, "needs a DG TVB_MLP context with a mesh and indicator weights");
+    const size_t ncell = (size_t)c->g.ny * c->g.nx;
+    float* dl = nullptr;
+    cudaError_t e = cudaMalloc(&dl, sizeof(float) * ncell);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dl, 0, sizeof(float) * ncell, c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_dg_tvb(c->opt.order, c->Un, true, c->kind, c->gsrc, c->g, c->da, c->gamma, c->opt.tvb_M,
+                              nullptr, static_cast<const zk::MlpWeights*>(c->mlp), nullptr, nullptr, dl, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(logits, dl, sizeof(float) * ncell, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (dl) cudaFree(dl);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }

@@ -9,6 +9,8 @@
 // means are never modified, so the sweep is race-free in place.  Compiled with
 // --fmad=false: the FP64 instantiation is bit-identical to the oracle's C
 // restatement (oracle/dg_oracle.c: limit_tvb_all).
+#include <cuda_bf16.h>
+
 #include "dg_common.cuh"
 #include "zk_internal.h"
 #include "zk_mlp.h"
@@ -114,55 +116,223 @@ struct TvbArgs {
     const MlpWeights* mlp;  // non-null: only cells the indicator flags are limited
     float* features;   // features mode: [ncell][40] output, no limiting
     uint32_t* nflag;   // count of limited cells, may be null
+    float* logits;     // with mlp: per-cell logit output [ny*nx], no limiting
 };
+
+// ---- indicator inference on the tensor cores --------------------------------------
+// One warp evaluates the MLP for its 32 cells with mma.sync m16n8k16 BF16
+// (FP32 accumulation): M = 32 cells (2 tiles), K = 48 (40 features, zero
+// padded) then 32, N = 32 hidden units (4 tiles).  A layer's accumulator tiles
+// are re-packed in registers as the next layer's A operand.
+constexpr int KP = 56;  // row stride (bf16) of the per-warp feature tile
+
+struct MlpSmem {
+    uint16_t w1[MLP_H][KP];  // bf16 bits, [out][in], in padded to 48 with zeros
+    uint16_t w2[MLP_H][40];
+    uint16_t w3[MLP_H][40];
+    float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H], b4;
+    uint16_t f[4][32][KP];   // per-warp feature tiles
+    float logit[4][32];
+};
+
+__device__ __forceinline__ uint16_t bf16_bits(float x) {
+    __nv_bfloat16 b = __float2bfloat16(x);
+    return *reinterpret_cast<uint16_t*>(&b);
+}
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    return (uint32_t)bf16_bits(lo) | ((uint32_t)bf16_bits(hi) << 16);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ void stage_mlp_weights(MlpSmem& S, const MlpWeights& W) {
+    for (int e = threadIdx.x; e < MLP_H * KP; e += blockDim.x) {
+        const int o = e / KP, i = e % KP;
+        S.w1[o][i] = bf16_bits(i < MLP_IN ? W.w1[o][i] : 0.0f);
+    }
+    for (int e = threadIdx.x; e < MLP_H * MLP_H; e += blockDim.x) {
+        const int o = e / MLP_H, i = e % MLP_H;
+        S.w2[o][i] = bf16_bits(W.w2[o][i]);
+        S.w3[o][i] = bf16_bits(W.w3[o][i]);
+    }
+    for (int o = threadIdx.x; o < MLP_H; o += blockDim.x) {
+        S.b1[o] = W.b1[o]; S.b2[o] = W.b2[o]; S.b3[o] = W.b3[o]; S.w4[o] = W.w4[o];
+    }
+    if (threadIdx.x == 0) S.b4 = W.b4;
+}
+
+// Hidden layer: acc[mt][nt][4] = A (from a-fragments) x W^T, + bias, GELU.
+template <int KSTEPS>
+__device__ __forceinline__ void mlp_layer(const uint32_t (&a)[2][KSTEPS][4], const uint16_t* w, int wstride,
+                                          const float* bias, float (&h)[2][4][4], int lane) {
+    const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) h[mt][nt][e] = 0.0f;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        const uint16_t* wr = w + (nt * 8 + g) * wstride;
+#pragma unroll
+        for (int kt = 0; kt < KSTEPS; ++kt) {
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 2 * q);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(wr + kt * 16 + 8 + 2 * q);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) mma_bf16(h[mt][nt], a[mt][kt][0], a[mt][kt][1], a[mt][kt][2], a[mt][kt][3], b0, b1);
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+        const float bl = bias[nt * 8 + 2 * q], bh = bias[nt * 8 + 2 * q + 1];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            h[mt][nt][0] = gelu(h[mt][nt][0] + bl);
+            h[mt][nt][1] = gelu(h[mt][nt][1] + bh);
+            h[mt][nt][2] = gelu(h[mt][nt][2] + bl);
+            h[mt][nt][3] = gelu(h[mt][nt][3] + bh);
+        }
+    }
+}
+
+// Accumulator tiles (m16n8, 4 of them along N) -> A fragments (m16k16, 2 k steps).
+__device__ __forceinline__ void repack(const float (&h)[2][4][4], uint32_t (&a)[2][2][4]) {
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int kt = 0; kt < 2; ++kt) {
+            a[mt][kt][0] = pack2(h[mt][2 * kt][0], h[mt][2 * kt][1]);
+            a[mt][kt][1] = pack2(h[mt][2 * kt][2], h[mt][2 * kt][3]);
+            a[mt][kt][2] = pack2(h[mt][2 * kt + 1][0], h[mt][2 * kt + 1][1]);
+            a[mt][kt][3] = pack2(h[mt][2 * kt + 1][2], h[mt][2 * kt + 1][3]);
+        }
+}
+
+// Logit of this lane's cell; every lane of the warp must call it.
+__device__ float mlp_logit_mma(MlpSmem& S, int warp, int lane, const float (&f)[MLP_IN]) {
+    uint16_t* row = S.f[warp][lane];
+#pragma unroll
+    for (int i = 0; i < MLP_IN; i += 2) *reinterpret_cast<uint32_t*>(row + i) = pack2(f[i], f[i + 1]);
+#pragma unroll
+    for (int i = MLP_IN; i < 48; i += 2) *reinterpret_cast<uint32_t*>(row + i) = 0u;
+    __syncwarp();
+    const int g = lane >> 2, q = lane & 3;
+    uint32_t a1[2][3][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int kt = 0; kt < 3; ++kt) {
+            const uint16_t* r0 = S.f[warp][mt * 16 + g] + kt * 16 + 2 * q;
+            const uint16_t* r1 = S.f[warp][mt * 16 + g + 8] + kt * 16 + 2 * q;
+            a1[mt][kt][0] = *reinterpret_cast<const uint32_t*>(r0);
+            a1[mt][kt][1] = *reinterpret_cast<const uint32_t*>(r1);
+            a1[mt][kt][2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+            a1[mt][kt][3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+        }
+    float h[2][4][4];
+    uint32_t a[2][2][4];
+    mlp_layer<3>(a1, &S.w1[0][0], KP, S.b1, h, lane);
+    repack(h, a);
+    mlp_layer<2>(a, &S.w2[0][0], 40, S.b2, h, lane);
+    repack(h, a);
+    mlp_layer<2>(a, &S.w3[0][0], 40, S.b3, h, lane);
+    // output unit: per row, sum over this lane's 8 columns, then over the quad
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        float lo = 0.0f, hi = 0.0f;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            const float w0 = S.w4[nt * 8 + 2 * q], w1 = S.w4[nt * 8 + 2 * q + 1];
+            lo = fmaf(w0, h[mt][nt][0], fmaf(w1, h[mt][nt][1], lo));
+            hi = fmaf(w0, h[mt][nt][2], fmaf(w1, h[mt][nt][3], hi));
+        }
+        lo += __shfl_xor_sync(0xffffffffu, lo, 1);
+        lo += __shfl_xor_sync(0xffffffffu, lo, 2);
+        hi += __shfl_xor_sync(0xffffffffu, hi, 1);
+        hi += __shfl_xor_sync(0xffffffffu, hi, 2);
+        if (q == 0) {
+            S.logit[warp][mt * 16 + g] = lo + S.b4;
+            S.logit[warp][mt * 16 + g + 8] = hi + S.b4;
+        }
+    }
+    __syncwarp();
+    return S.logit[warp][lane];
+}
 
 template <typename T, int P>
 __global__ void __launch_bounds__(128) tvb_kernel(TvbArgs a) {
     constexpr int NM = (P + 1) * (P + 1);
+    __shared__ __align__(16) MlpSmem S;
+    const bool gated = a.mlp != nullptr;  // uniform over the grid
+    if (gated) {
+        stage_mlp_weights(S, *a.mlp);
+        __syncthreads();
+    }
     const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
-    if (j >= a.g.nx || i >= a.g.ny) return;
-    const size_t k = (size_t)i * a.g.pitch + j, plane = a.g.plane, vs = (size_t)NM * plane;
+    const bool inside = j < a.g.nx && i < a.g.ny;
+    const size_t k = inside ? (size_t)i * a.g.pitch + j : 0;
+    const size_t plane = a.g.plane, vs = (size_t)NM * plane;
     T* d = static_cast<T*>(a.state);
-    if (a.flags) a.flags[k] = 0;
-    if ((a.kind[k] & KIND_MASK) != KIND_UPDATED) return;
-    const int nx = a.g.nx;
-    T ub[4], uL[4], uR[4], uU[4], uD[4];
+    if (inside && a.flags) a.flags[k] = 0;
+    const bool active = inside && (a.kind[k] & KIND_MASK) == KIND_UPDATED;
+    if (!gated && !active) return;  // ungated: no warp-wide work follows
+    T ub[4] = {T(0), T(0), T(0), T(0)}, uL[4] = {T(0), T(0), T(0), T(0)}, uR[4] = {T(0), T(0), T(0), T(0)},
+      uU[4] = {T(0), T(0), T(0), T(0)}, uD[4] = {T(0), T(0), T(0), T(0)};
+    if (active) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) ub[c] = d[(size_t)c * vs + k];
-    nb_mean<T>(d, a.kind, a.gsrc, k - 1, vs, uL);
-    nb_mean<T>(d, a.kind, a.gsrc, k + 1, vs, uR);
-    nb_mean<T>(d, a.kind, a.gsrc, k - (size_t)a.g.pitch, vs, uU);
-    nb_mean<T>(d, a.kind, a.gsrc, k + (size_t)a.g.pitch, vs, uD);
-    (void)nx;
-    if (a.features || a.mlp) {
+        for (int c = 0; c < 4; ++c) ub[c] = d[(size_t)c * vs + k];
+        nb_mean<T>(d, a.kind, a.gsrc, k - 1, vs, uL);
+        nb_mean<T>(d, a.kind, a.gsrc, k + 1, vs, uR);
+        nb_mean<T>(d, a.kind, a.gsrc, k - (size_t)a.g.pitch, vs, uU);
+        nb_mean<T>(d, a.kind, a.gsrc, k + (size_t)a.g.pitch, vs, uD);
+    }
+    if (a.features || gated) {
         float f[MLP_IN];
-        // rho and E modes, slot px*4+py, scaled by the largest |mean| around
-        const float sr = (float)tmax_(tmax_(tmax_(fabs(ub[0]), fabs(uL[0])), tmax_(fabs(uR[0]), fabs(uU[0]))),
-                                      fabs(uD[0])) + 1e-12f;
-        const float se = (float)tmax_(tmax_(tmax_(fabs(ub[3]), fabs(uL[3])), tmax_(fabs(uR[3]), fabs(uU[3]))),
-                                      fabs(uD[3])) + 1e-12f;
 #pragma unroll
-        for (int s = 0; s < 16; ++s) { f[s] = 0.0f; f[16 + s] = 0.0f; }
+        for (int s = 0; s < MLP_IN; ++s) f[s] = 0.0f;
+        if (active) {
+            // rho and E modes, slot px*4+py, scaled by the largest |mean| around
+            const float sr = (float)tmax_(tmax_(tmax_(fabs(ub[0]), fabs(uL[0])), tmax_(fabs(uR[0]), fabs(uU[0]))),
+                                          fabs(uD[0])) + 1e-12f;
+            const float se = (float)tmax_(tmax_(tmax_(fabs(ub[3]), fabs(uL[3])), tmax_(fabs(uR[3]), fabs(uU[3]))),
+                                          fabs(uD[3])) + 1e-12f;
 #pragma unroll
-        for (int m = 0; m < NM; ++m) {
-            const int slot = (m / (P + 1)) * 4 + m % (P + 1);
-            f[slot] = (float)d[(size_t)m * plane + k] / sr;
-            f[16 + slot] = (float)d[3 * vs + (size_t)m * plane + k] / se;
-        }
-        const T* nb[4] = {uL, uR, uU, uD};
+            for (int m = 0; m < NM; ++m) {
+                const int slot = (m / (P + 1)) * 4 + m % (P + 1);
+                f[slot] = (float)d[(size_t)m * plane + k] / sr;
+                f[16 + slot] = (float)d[3 * vs + (size_t)m * plane + k] / se;
+            }
+            const T* nb[4] = {uL, uR, uU, uD};
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-            f[32 + n] = (float)(nb[n][0] - ub[0]) / sr;
-            f[36 + n] = (float)(nb[n][3] - ub[3]) / se;
+            for (int n = 0; n < 4; ++n) {
+                f[32 + n] = (float)(nb[n][0] - ub[0]) / sr;
+                f[36 + n] = (float)(nb[n][3] - ub[3]) / se;
+            }
         }
         if (a.features) {
-            const size_t cell = (size_t)i * a.g.nx + j;
+            if (active) {
+                const size_t cell = (size_t)i * a.g.nx + j;
 #pragma unroll
-            for (int s = 0; s < MLP_IN; ++s) a.features[cell * MLP_IN + s] = f[s];
-        } else if (mlp_logit(*a.mlp, f) <= 0.0f) {
-            return;  // indicator says smooth: skip the characteristic branch
+                for (int s = 0; s < MLP_IN; ++s) a.features[cell * MLP_IN + s] = f[s];
+            }
+        } else {
+            const float z = mlp_logit_mma(S, threadIdx.x >> 5, threadIdx.x & 31, f);
+            if (a.logits) {
+                if (active) a.logits[(size_t)i * a.g.nx + j] = z;
+                return;
+            }
+            if (!(z > 0.0f)) return;  // indicator says smooth: skip the characteristic branch
         }
     }
+    if (!active) return;
     const T mh2 = T(a.M) * T(a.da) * T(a.da);
     T ax[4], ay[4], dxp[4], dxm[4], dyp[4], dym[4], lx[4], ly[4];
 #pragma unroll
@@ -206,8 +376,8 @@ cudaError_t launch_t(int P, const TvbArgs& a, cudaStream_t s) {
 
 cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
                           double da, double gamma, double M, uint8_t* flags, const MlpWeights* mlp,
-                          float* features, uint32_t* nflag, cudaStream_t s) {
-    TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, mlp, features, nflag};
+                          float* features, uint32_t* nflag, float* logits, cudaStream_t s) {
+    TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, mlp, features, nflag, logits};
     return fp64 ? launch_t<double>(P, a, s) : launch_t<float>(P, a, s);
 }
 
