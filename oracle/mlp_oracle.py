@@ -44,17 +44,17 @@ def init_params(seed: int = 0) -> np.ndarray:
     return np.concatenate([np.ravel(a) for a in parts]).astype(np.float32)
 
 
-def _erf(x):
-    from scipy.special import erf
-    return erf(x)
+_K, _C = math.sqrt(2.0 / math.pi), 0.044715
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + _erf(x / math.sqrt(2.0)))
+    """GELU, tanh form (the form the GPU kernels use)."""
+    return 0.5 * x * (1.0 + np.tanh(_K * (x + _C * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + _erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(_K * (x + _C * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * _K * (1.0 + 3.0 * _C * x * x)
 
 
 def forward(p, X):

@@ -195,10 +195,10 @@ __device__ __forceinline__ void mlp_layer(const uint32_t (&a)[2][KSTEPS][4], con
         const float bl = bias[nt * 8 + 2 * q], bh = bias[nt * 8 + 2 * q + 1];
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
-            h[mt][nt][0] = gelu(h[mt][nt][0] + bl);
-            h[mt][nt][1] = gelu(h[mt][nt][1] + bh);
-            h[mt][nt][2] = gelu(h[mt][nt][2] + bl);
-            h[mt][nt][3] = gelu(h[mt][nt][3] + bh);
+            h[mt][nt][0] = gelu_fast(h[mt][nt][0] + bl);
+            h[mt][nt][1] = gelu_fast(h[mt][nt][1] + bh);
+            h[mt][nt][2] = gelu_fast(h[mt][nt][2] + bl);
+            h[mt][nt][3] = gelu_fast(h[mt][nt][3] + bh);
         }
     }
 }
@@ -267,16 +267,26 @@ __device__ float mlp_logit_mma(MlpSmem& S, int warp, int lane, const float (&f)[
     return S.logit[warp][lane];
 }
 
+constexpr int kTvbRows = 8;  // rows per CTA (the indicator's weights are staged once per CTA)
+
+template <typename T, int P>
+__device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gated, int i, int j);
+
 template <typename T, int P>
 __global__ void __launch_bounds__(128) tvb_kernel(TvbArgs a) {
-    constexpr int NM = (P + 1) * (P + 1);
     __shared__ __align__(16) MlpSmem S;
     const bool gated = a.mlp != nullptr;  // uniform over the grid
     if (gated) {
         stage_mlp_weights(S, *a.mlp);
         __syncthreads();
     }
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int r = 0; r < kTvbRows; ++r) tvb_cell<T, P>(a, S, gated, blockIdx.y * kTvbRows + r, j);
+}
+
+template <typename T, int P>
+__device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gated, int i, int j) {
+    constexpr int NM = (P + 1) * (P + 1);
     const bool inside = j < a.g.nx && i < a.g.ny;
     const size_t k = inside ? (size_t)i * a.g.pitch + j : 0;
     const size_t plane = a.g.plane, vs = (size_t)NM * plane;
@@ -362,7 +372,7 @@ __global__ void __launch_bounds__(128) tvb_kernel(TvbArgs a) {
 
 template <typename T>
 cudaError_t launch_t(int P, const TvbArgs& a, cudaStream_t s) {
-    dim3 grid((a.g.nx + 127) / 128, a.g.ny);
+    dim3 grid((a.g.nx + 127) / 128, (a.g.ny + kTvbRows - 1) / kTvbRows);
     switch (P) {
         case 1: tvb_kernel<T, 1><<<grid, 128, 0, s>>>(a); break;
         case 2: tvb_kernel<T, 2><<<grid, 128, 0, s>>>(a); break;

@@ -29,10 +29,10 @@ constexpr int H = MLP_H, IN = MLP_IN, NP = MLP_NPARAM;
 constexpr int OW1 = 0, OB1 = OW1 + H * IN, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H, OB3 = OW3 + H * H,
               OW4 = OB3 + H, OB4 = OW4 + H;
 
+// d/dx of the tanh-form GELU.
 __device__ __forceinline__ float gelu_grad(float x) {
-    const float cdf = 0.5f * (1.0f + erff(x * 0.70710678118654752f));
-    const float pdf = 0.3989422804014327f * expf(-0.5f * x * x);
-    return cdf + x * pdf;
+    const float t = tanhf(GELU_K * (x + GELU_C * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_K * (1.0f + 3.0f * GELU_C * x * x);
 }
 
 struct SmemFB {

@@ -29,7 +29,18 @@ struct MlpWeights {
 };
 static_assert(sizeof(MlpWeights) == sizeof(float) * MLP_NPARAM, "MlpWeights must be a flat float block");
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
+constexpr float GELU_K = 0.7978845608028654f, GELU_C = 0.044715f;
+__device__ __forceinline__ float gelu(float x) {
+    return 0.5f * x * (1.0f + tanhf(GELU_K * (x + GELU_C * x * x * x)));
+}
+// The same with the hardware tanh approximation (inference).
+__device__ __forceinline__ float gelu_fast(float x) {
+    float t;
+    const float u = GELU_K * (x + GELU_C * x * x * x);
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+    return 0.5f * x * (1.0f + t);
+}
 
 // Plain FP32 forward pass (CUDA cores).
 __device__ __forceinline__ float mlp_logit(const MlpWeights& W, const float f[MLP_IN]) {
