@@ -267,7 +267,7 @@ __device__ float mlp_logit_mma(MlpSmem& S, int warp, int lane, const float (&f)[
     return S.logit[warp][lane];
 }
 
-constexpr int kTvbRows = 8;  // rows per CTA (the indicator's weights are staged once per CTA)
+constexpr int kTvbRows = 1;  // rows per CTA
 
 template <typename T, int P>
 __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gated, int i, int j);
