@@ -124,11 +124,12 @@ def features(P: int, dof: np.ndarray, kind: np.ndarray, src: np.ndarray) -> np.n
         nb = [mean(k - 1), mean(k + 1), mean(k - nx), mean(k + nx)]
         sr = np.float32(max(abs(ub[0]), *(abs(v[0]) for v in nb))) + np.float32(1e-12)
         se = np.float32(max(abs(ub[3]), *(abs(v[3]) for v in nb))) + np.float32(1e-12)
+        ir, ie = np.float32(1.0) / sr, np.float32(1.0) / se
         for m in range(NM):
             slot = (m // (P + 1)) * 4 + m % (P + 1)
-            out[k, slot] = np.float32(flat[0, m, k]) / sr
-            out[k, 16 + slot] = np.float32(flat[3, m, k]) / se
+            out[k, slot] = np.float32(flat[0, m, k]) * ir
+            out[k, 16 + slot] = np.float32(flat[3, m, k]) * ie
         for n_, v in enumerate(nb):
-            out[k, 32 + n_] = np.float32(v[0] - ub[0]) / sr
-            out[k, 36 + n_] = np.float32(v[3] - ub[3]) / se
+            out[k, 32 + n_] = np.float32(v[0] - ub[0]) * ir
+            out[k, 36 + n_] = np.float32(v[3] - ub[3]) * ie
     return out

@@ -1,6 +1,7 @@
 // DG driver: buffers, tables and the SSP-RK3 stage sequence of updateMesh
 // (src_DG/fluid.cpp:1005-1054) on the device state.
 #include <cmath>
+#include <cstring>
 
 #include <vector>
 
@@ -15,7 +16,7 @@ cudaError_t launch_dg_stage_fp64(int P, const DGArgs& a, cudaStream_t s);
 cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s);
 int dg_upload_tables_f32(int P);
 cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
-                          double da, double gamma, double M, uint8_t* flags, const MlpWeights* mlp,
+                          double da, double gamma, double M, uint8_t* flags, const MlpPacked* mlp,
                           float* features, uint32_t* nflag, float* logits, cudaStream_t s);
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
@@ -90,7 +91,7 @@ int zk_dg_setup(zk_ctx* c) {
     if (e == cudaSuccess && !c->d_nflag) e = cudaMalloc(&c->d_nflag, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_nflag, 0, sizeof(uint32_t), c->stream);
     if (e == cudaSuccess && c->opt.limiter == ZK_LIMITER_TVB_MLP && !c->mlp)
-        e = cudaMalloc(&c->mlp, sizeof(zk::MlpWeights));
+        e = cudaMalloc(&c->mlp, sizeof(zk::MlpPacked));
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }
@@ -98,10 +99,10 @@ int zk_dg_setup(zk_ctx* c) {
 // TVB pass (plain or indicator-gated) on a stage output, when configured.
 int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64) {
     if (c->opt.limiter < ZK_LIMITER_TVB) return ZK_OK;
-    const zk::MlpWeights* w = nullptr;
+    const zk::MlpPacked* w = nullptr;
     if (c->opt.limiter == ZK_LIMITER_TVB_MLP) {
         if (!c->mlp_set) return zk_internal_fail(ZK_ERR_STATE, "indicator weights not set (zk_set_indicator)");
-        w = static_cast<const zk::MlpWeights*>(c->mlp);
+        w = static_cast<const zk::MlpPacked*>(c->mlp);
     }
     cudaError_t e = zk::launch_dg_tvb(c->opt.order, state, fp64, c->kind, c->gsrc, c->g, c->da, c->gamma,
                                       c->opt.tvb_M, c->d_flags, w, nullptr, c->d_nflag, nullptr, c->stream);
@@ -172,9 +173,28 @@ extern "C" int zk_set_indicator(zk_ctx* c, const float* params, int nparams) {
     if (nparams != zk::MLP_NPARAM) return zk_internal_fail(ZK_ERR_ARG, "indicator needs exactly MLP_NPARAM parameters");
     if (c->opt.limiter != ZK_LIMITER_TVB_MLP || !c->mlp)
         return zk_internal_fail(ZK_ERR_STATE, "context is not a DG TVB_MLP context with a mesh");
-    std::vector<float> w(params, params + nparams);
-    for (float& x : w) x = __bfloat162float(__float2bfloat16(x));  // BF16 inference weights
-    cudaError_t e = cudaMemcpyAsync(c->mlp, w.data(), sizeof(float) * nparams, cudaMemcpyHostToDevice, c->stream);
+    // BF16 inference weights, packed in the shared-memory layout of the
+    // tensor-core inference (zk_mlp.h: MlpPacked)
+    zk::MlpWeights W;
+    std::memcpy(&W, params, sizeof W);
+    zk::MlpPacked K;
+    std::memset(&K, 0, sizeof K);
+    auto bits = [](float x) {
+        __nv_bfloat16 b = __float2bfloat16(x);
+        uint16_t u;
+        std::memcpy(&u, &b, 2);
+        return u;
+    };
+    for (int o = 0; o < zk::MLP_H; ++o) {
+        for (int i = 0; i < zk::MLP_IN; ++i) K.w1[o][i] = bits(W.w1[o][i]);
+        for (int i = 0; i < zk::MLP_H; ++i) {
+            K.w2[o][i] = bits(W.w2[o][i]);
+            K.w3[o][i] = bits(W.w3[o][i]);
+        }
+        K.b1[o] = W.b1[o]; K.b2[o] = W.b2[o]; K.b3[o] = W.b3[o]; K.w4[o] = W.w4[o];
+    }
+    K.b4 = W.b4;
+    cudaError_t e = cudaMemcpyAsync(c->mlp, &K, sizeof K, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(e);
     c->mlp_set = true;
@@ -218,7 +238,7 @@ extern "C" int zk_indicator_logits(zk_ctx* c, float* logits) {
     if (e == cudaSuccess) e = cudaMemsetAsync(dl, 0, sizeof(float) * ncell, c->stream);
     if (e == cudaSuccess)
         e = zk::launch_dg_tvb(c->opt.order, c->Un, true, c->kind, c->gsrc, c->g, c->da, c->gamma, c->opt.tvb_M,
-                              nullptr, static_cast<const zk::MlpWeights*>(c->mlp), nullptr, nullptr, dl, c->stream);
+                              nullptr, static_cast<const zk::MlpPacked*>(c->mlp), nullptr, nullptr, dl, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(logits, dl, sizeof(float) * ncell, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (dl) cudaFree(dl);

@@ -113,7 +113,7 @@ struct TvbArgs {
     Grid g;
     double da, gamma, M;
     uint8_t* flags;    // per cell (pitched), may be null
-    const MlpWeights* mlp;  // non-null: only cells the indicator flags are limited
+    const MlpPacked* mlp;  // non-null: only cells the indicator flags are limited
     float* features;   // features mode: [ncell][40] output, no limiting
     uint32_t* nflag;   // count of limited cells, may be null
     float* logits;     // with mlp: per-cell logit output [ny*nx], no limiting
@@ -124,14 +124,11 @@ struct TvbArgs {
 // (FP32 accumulation): M = 32 cells (2 tiles), K = 48 (40 features, zero
 // padded) then 32, N = 32 hidden units (4 tiles).  A layer's accumulator tiles
 // are re-packed in registers as the next layer's A operand.
-constexpr int KP = 56;  // row stride (bf16) of the per-warp feature tile
+constexpr int KP = MLP_KP1;  // row stride (bf16) of the per-warp feature tile
 
 struct MlpSmem {
-    uint16_t w1[MLP_H][KP];  // bf16 bits, [out][in], in padded to 48 with zeros
-    uint16_t w2[MLP_H][40];
-    uint16_t w3[MLP_H][40];
-    float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H], b4;
-    uint16_t f[4][32][KP];   // per-warp feature tiles
+    MlpPacked w;
+    uint16_t f[4][32][KP];  // per-warp feature tiles
     float logit[4][32];
 };
 
@@ -152,20 +149,10 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__device__ void stage_mlp_weights(MlpSmem& S, const MlpWeights& W) {
-    for (int e = threadIdx.x; e < MLP_H * KP; e += blockDim.x) {
-        const int o = e / KP, i = e % KP;
-        S.w1[o][i] = bf16_bits(i < MLP_IN ? W.w1[o][i] : 0.0f);
-    }
-    for (int e = threadIdx.x; e < MLP_H * MLP_H; e += blockDim.x) {
-        const int o = e / MLP_H, i = e % MLP_H;
-        S.w2[o][i] = bf16_bits(W.w2[o][i]);
-        S.w3[o][i] = bf16_bits(W.w3[o][i]);
-    }
-    for (int o = threadIdx.x; o < MLP_H; o += blockDim.x) {
-        S.b1[o] = W.b1[o]; S.b2[o] = W.b2[o]; S.b3[o] = W.b3[o]; S.w4[o] = W.w4[o];
-    }
-    if (threadIdx.x == 0) S.b4 = W.b4;
+__device__ void stage_mlp_weights(MlpSmem& S, const MlpPacked& W) {
+    const uint4* src = reinterpret_cast<const uint4*>(&W);
+    uint4* dst = reinterpret_cast<uint4*>(&S.w);
+    for (int e = threadIdx.x; e < (int)(sizeof(MlpPacked) / 16); e += blockDim.x) dst[e] = src[e];
 }
 
 // Hidden layer: acc[mt][nt][4] = A (from a-fragments) x W^T, + bias, GELU.
@@ -239,18 +226,18 @@ __device__ float mlp_logit_mma(MlpSmem& S, int warp, int lane, const float (&f)[
         }
     float h[2][4][4];
     uint32_t a[2][2][4];
-    mlp_layer<3>(a1, &S.w1[0][0], KP, S.b1, h, lane);
+    mlp_layer<3>(a1, &S.w.w1[0][0], MLP_KP1, S.w.b1, h, lane);
     repack(h, a);
-    mlp_layer<2>(a, &S.w2[0][0], 40, S.b2, h, lane);
+    mlp_layer<2>(a, &S.w.w2[0][0], MLP_KP2, S.w.b2, h, lane);
     repack(h, a);
-    mlp_layer<2>(a, &S.w3[0][0], 40, S.b3, h, lane);
+    mlp_layer<2>(a, &S.w.w3[0][0], MLP_KP2, S.w.b3, h, lane);
     // output unit: per row, sum over this lane's 8 columns, then over the quad
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt) {
         float lo = 0.0f, hi = 0.0f;
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            const float w0 = S.w4[nt * 8 + 2 * q], w1 = S.w4[nt * 8 + 2 * q + 1];
+            const float w0 = S.w.w4[nt * 8 + 2 * q], w1 = S.w.w4[nt * 8 + 2 * q + 1];
             lo = fmaf(w0, h[mt][nt][0], fmaf(w1, h[mt][nt][1], lo));
             hi = fmaf(w0, h[mt][nt][2], fmaf(w1, h[mt][nt][3], hi));
         }
@@ -259,8 +246,8 @@ __device__ float mlp_logit_mma(MlpSmem& S, int warp, int lane, const float (&f)[
         hi += __shfl_xor_sync(0xffffffffu, hi, 1);
         hi += __shfl_xor_sync(0xffffffffu, hi, 2);
         if (q == 0) {
-            S.logit[warp][mt * 16 + g] = lo + S.b4;
-            S.logit[warp][mt * 16 + g + 8] = hi + S.b4;
+            S.logit[warp][mt * 16 + g] = lo + S.w.b4;
+            S.logit[warp][mt * 16 + g + 8] = hi + S.w.b4;
         }
     }
     __syncwarp();
@@ -314,17 +301,18 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
                                           fabs(uD[0])) + 1e-12f;
             const float se = (float)tmax_(tmax_(tmax_(fabs(ub[3]), fabs(uL[3])), tmax_(fabs(uR[3]), fabs(uU[3]))),
                                           fabs(uD[3])) + 1e-12f;
+            const float ir = 1.0f / sr, ie = 1.0f / se;
 #pragma unroll
             for (int m = 0; m < NM; ++m) {
                 const int slot = (m / (P + 1)) * 4 + m % (P + 1);
-                f[slot] = (float)d[(size_t)m * plane + k] / sr;
-                f[16 + slot] = (float)d[3 * vs + (size_t)m * plane + k] / se;
+                f[slot] = (float)d[(size_t)m * plane + k] * ir;
+                f[16 + slot] = (float)d[3 * vs + (size_t)m * plane + k] * ie;
             }
             const T* nb[4] = {uL, uR, uU, uD};
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
-                f[32 + n] = (float)(nb[n][0] - ub[0]) / sr;
-                f[36 + n] = (float)(nb[n][3] - ub[3]) / se;
+                f[32 + n] = (float)(nb[n][0] - ub[0]) * ir;
+                f[36 + n] = (float)(nb[n][3] - ub[3]) * ie;
             }
         }
         if (a.features) {
@@ -385,7 +373,7 @@ cudaError_t launch_t(int P, const TvbArgs& a, cudaStream_t s) {
 }  // namespace
 
 cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
-                          double da, double gamma, double M, uint8_t* flags, const MlpWeights* mlp,
+                          double da, double gamma, double M, uint8_t* flags, const MlpPacked* mlp,
                           float* features, uint32_t* nflag, float* logits, cudaStream_t s) {
     TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, mlp, features, nflag, logits};
     return fp64 ? launch_t<double>(P, a, s) : launch_t<float>(P, a, s);

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cstdint>
 
 namespace zk {
 
@@ -28,6 +29,19 @@ struct MlpWeights {
     float b4;
 };
 static_assert(sizeof(MlpWeights) == sizeof(float) * MLP_NPARAM, "MlpWeights must be a flat float block");
+
+// Inference copy of the weights, packed on the host in the exact shared-memory
+// layout of the tensor-core inference (BF16 bits, rows padded for mma
+// fragment loads), so a CTA stages it with 16-byte vector copies.
+constexpr int MLP_KP1 = 56, MLP_KP2 = 40;
+struct MlpPacked {
+    uint16_t w1[MLP_H][MLP_KP1];  // [out][in], in 40..55 zero
+    uint16_t w2[MLP_H][MLP_KP2];  // [out][in], in 32..39 zero
+    uint16_t w3[MLP_H][MLP_KP2];
+    float b1[MLP_H], b2[MLP_H], b3[MLP_H], w4[MLP_H];
+    float b4, pad[3];
+};
+static_assert(sizeof(MlpPacked) % 16 == 0, "MlpPacked is copied in 16-byte units");
 
 // GELU in its tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))).
 constexpr float GELU_K = 0.7978845608028654f, GELU_C = 0.044715f;
