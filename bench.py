@@ -66,17 +66,20 @@ def make_workload(name: str, rank: int):
         c = cases.four_quadrant(n, seed=seed)
         lam = c.da / cases.cfl_dt(c, 1.0)
         dt = 0.5 * 0.9 / (2.0 * (2 * P + 1)) * c.da / lam
+        learned = P == 3
         return dict(case=c, method="dg", order=P, dof_per_cell=4 * (P + 1) ** 2, dt=dt,
-                    opts={"limiter": "reference"},
+                    opts={"fp64": {"limiter": "tvb"}, "mixed": {"limiter": "tvb_mlp" if learned else "tvb"}},
                     desc=f"seeded four-quadrant Riemann {n}x{n} (seed {seed}), DG P={P} HLLC SSP-RK3, "
-                         f"Persson+Zhang-Shu limiter, half the reference's CFL limit")
+                         + ("mixed precision + learned troubled-cell indicator gating TVB (M=50) limiting vs "
+                            "plain FP64 + TVB limiting" if learned else "TVB limiter M=50")
+                         + ", half the reference's CFL limit")
     if name.startswith("dg") and "_wave_" in name:
         P = int(name[2])
         n = int(name.split("_")[-1])
         c = cases.smooth_wave(n)
         dt = 0.9 / (2.0 * (2 * P + 1)) * c.da / 2.74
         return dict(case=c, method="dg", order=P, dof_per_cell=4 * (P + 1) ** 2, dt=dt,
-                    opts={"limiter": "none", "boundary": "periodic"},
+                    opts={"limiter": "tvb", "boundary": "periodic"},
                     desc=f"periodic smooth wave {n}^2 on [0,2]^2, DG P={P} HLLC SSP-RK3, dt at the reference's CFL limit")
     raise SystemExit(f"unknown workload {name}")
 
@@ -281,7 +284,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="weno_fq_2048")
+    ap.add_argument("--workload", default="dg3_fq_2048")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--fp64-only", action="store_true", help="time the FP64 path only")
@@ -319,6 +322,14 @@ def main():
                        "value": world * dofs * args.steps / (ms_max * 1e-3), "solver": s}
     head = "mixed" if "mixed" in paths else "fp64"
     hp = paths[head]
+    # equal-L1 diagnostic: both paths advanced the same steps from the same
+    # state; relative L1 difference of the cell-average density
+    eq = None
+    if "mixed" in paths:
+        r64 = paths["fp64"]["solver"].recover_primitives()[0]
+        rmx = paths["mixed"]["solver"].recover_primitives()[0]
+        eq = {"rel_l1_density_mixed_vs_fp64": float(np.abs(rmx - r64).sum() / np.abs(r64).sum()),
+              "steps_compared": args.warmup + args.steps}
 
     # end to end through the public API with host buffers: the reference
     # driver's loop (computeMaxSpeed -> dt on the host -> updateMesh), state
@@ -365,10 +376,10 @@ def main():
                           "l2": "working set (3 FP64 states = %.0f MB) larger than the 126 MB L2" %
                                 (3 * U0.nbytes / 1e6),
                           "parallelism": f"replicas x{world} (independent seeded problems)"},
-               "fp64_value": paths["fp64"]["value"],
+               "fp64_value": paths["fp64"]["value"], "equal_l1": eq,
                "speedup_vs_fp64": hp["value"] / paths["fp64"]["value"],
                "clocks": hp["clocks"], "e2e": e2e,
-               "gpu_launches": 3 * args.steps if (w["method"] == "weno" or head == "mixed") else 9 * args.steps,
+               "gpu_launches": gpu_launches(w, head) * args.steps,
                "roofline": roofs[head], "roofline_fp64": roofs["fp64"], "cpu_baseline": cpu,
                "status_word": {p: v["status"] for p, v in paths.items()}, "peaks": peaks}
         print(json.dumps(out), flush=True)
@@ -378,10 +389,24 @@ def main():
         pg.destroy_process_group()
 
 
+def gpu_launches(w, prec) -> int:
+    """Kernels of this library launched per step on the headline path."""
+    if w["method"] == "weno":
+        return 3
+    per_stage = 1 if prec == "mixed" else 3
+    lim = (w["opts"].get(prec, {}) if "fp64" in w["opts"] else w["opts"]).get("limiter", "reference")
+    return 3 * (per_stage + (1 if lim in ("tvb", "tvb_mlp") else 0))
+
+
 def open_solver(w, c, U0, precision, device):
-    from zuikakucfd_b200 import Solver
-    s = Solver(method=w["method"], order=max(w["order"], 1), precision=precision, device=device, **w["opts"])
+    import ctypes as C
+    from zuikakucfd_b200 import Solver, _native as N, indicator
+    opts = w["opts"].get(precision, w["opts"]) if "fp64" in w["opts"] else w["opts"]
+    s = Solver(method=w["method"], order=max(w["order"], 1), precision=precision, device=device, **opts)
     s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
+    if opts.get("limiter") == "tvb_mlp":
+        wts = indicator.load()
+        N.check(N.lib().zk_set_indicator(s._h, wts.ctypes.data_as(C.POINTER(C.c_float)), wts.size))
     s.set_state(U0)
     return s
 
