@@ -101,10 +101,12 @@ def test_dg_p3_full_size_determinism():
     assert np.isfinite(outs[0]).all()
 
 
-def test_dg_unsupported_options_fail_loudly():
+def test_dg_bad_options_fail_loudly():
     from zuikakucfd_b200 import Solver
     from zuikakucfd_b200._native import ZkError
     b = np.zeros((16, 16), np.int32)
-    with Solver(method="dg", order=2, limiter="tvb") as s:
-        with pytest.raises(ZkError, match="UNSUPPORTED"):
+    with Solver(method="dg", order=2, limiter="tvb", tvb_M=-1.0) as s:
+        with pytest.raises(ZkError, match="ZK_ERR_ARG"):
             s.set_mesh(16, 16, 0.1, 1.4, b)
+    with pytest.raises(ZkError, match="ZK_ERR_ARG"):
+        Solver(method="dg", order=4)
