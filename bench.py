@@ -288,11 +288,22 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--fp64-only", action="store_true", help="time the FP64 path only")
+    ap.add_argument("--batch-policies", default="all,sjf",
+                    help="batch workloads: admission policies to run (the first of 'all' or the list is the value)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     rank, world, local, pg = dist_setup(args.gpus)
+    if args.workload.startswith("batch"):
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps(run_reference_batch(args)), flush=True)
+        else:
+            run_batch(args, rank, local, world, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference_arm(args, make_workload(args.workload, 0))), flush=True)
@@ -387,6 +398,151 @@ def main():
         pth["solver"].close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def parse_batch(name: str) -> tuple[int, int]:
+    """batch<N>[_s<steps>]: N problems (default workload: 256), steps each (500)."""
+    head, _, tail = name.partition("_s")
+    return int(head[len("batch"):] or 256), int(tail or 500)
+
+
+def batch_cpu_rates(seconds: float = 8.0) -> dict:
+    """Reference CPU seconds per cell-step of WENO5 and of DG P=2 (its own
+    Persson + Zhang-Shu limiter), each timed on a bounded strip of a 1024^2
+    four-quadrant problem with x-slab threads on this host's cores."""
+    from oracle.oracle import Reference, reference_available
+    from zuikakucfd_b200 import cases
+    if not reference_available("faithful"):
+        return {}
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    R = Reference("faithful")
+    out = {"cores": cores}
+    c = cases.four_quadrant(1024, seed=7)
+    lam = c.da / cases.cfl_dt(c, 1.0)
+    for key, w in (("weno", dict(case=c, method="weno", order=0, dt=0.4 * c.da / lam)),
+                   ("dg2", dict(case=c, method="dg", order=2, dt=0.5 * 0.9 / 10.0 * c.da / lam))):
+        st, b, rows = _ref_strip(R, w, cores, 1000.0)
+        ms, cells = _ref_slabs(R, w, st, b, 1, cores)
+        n = max(1, int(seconds * 1e3 / max(ms, 1.0)))
+        ms, cells = _ref_slabs(R, w, st, b, n, cores)
+        out[key] = ms * 1e-3 / (cells * n)
+        out[key + "_sample"] = f"{n} x updateMesh on a {rows}x1024 strip, {cores} x-slab threads"
+    return out
+
+
+def run_batch(args, rank: int, local: int, world: int, pg) -> None:
+    """Batched serving (one step = one SSP-RK3 step of every running problem):
+    N seeded four-quadrant problems, sides uniform in {128, ..., 1024}, half
+    WENO5 / half DG P=2, mixed precision, each run `steps` steps at its own CFL
+    dt, all through zk_batch (persistent launches, graph-captured steps,
+    autotuned tiles).  value = aggregate DOF-updates/s (device time of the run,
+    policy "all"); latencies p50/p99 for both admission policies."""
+    import torch
+    from zuikakucfd_b200.batch import Batch, batch_problems
+    nprob, nsteps = parse_batch(args.workload)
+    specs = list(batch_problems(nprob, seed=1000 + rank, nsteps=nsteps))
+    # pinned host copies of every initial state (the e2e leg uploads from these)
+    pinned = [torch.from_numpy(np.ascontiguousarray(s["state"])).pin_memory() for s in specs]
+    for s, p in zip(specs, pinned):
+        s["state"] = p.numpy()
+    in_bytes = sum(p.numel() * 8 for p in pinned)
+    cells = sum(int((s["bctype"][3:-3, 3:-3] == 0).sum()) for s in specs)
+    # warm-up: the same problems for 3 steps (autotunes every group once; the
+    # choice is cached for the process)
+    with Batch(policy="all", graph_steps=10, device=local) as b:
+        for s in specs:
+            b.add(**{**s, "nsteps": 3})
+        b.run()
+    results = {}
+    for policy in args.batch_policies.split(","):
+        barrier(pg)
+        with Batch(policy=policy, graph_steps=10, device=local) as b:
+            t0 = time.perf_counter()
+            ids = [b.add(**s) for s in specs]
+            with ClockSampler(local) as clk:
+                rep = b.run()
+            outs = {}
+            for i in ids:  # read every final state back (one buffer per shape)
+                shp = b._shapes[i]
+                buf = outs.setdefault(shp, torch.empty(shp, dtype=torch.float64).pin_memory())
+                from zuikakucfd_b200 import _native as N
+                import ctypes as C
+                N.check(N.lib().zk_batch_get_state(b._h, i, C.cast(buf.data_ptr(), C.POINTER(C.c_double))))
+            wall = time.perf_counter() - t0
+            groups = b.groups()
+        results[policy] = {"rep": rep, "wall": wall, "clocks": clk.summary(), "groups": groups}
+    head = results.get("all") or next(iter(results.values()))
+    rep = head["rep"]
+    ms = allreduce_max(pg, rep["ms"])
+    wall = allreduce_max(pg, head["wall"])
+    if rank != 0:
+        return
+    peaks = measure_peaks(local)
+    flops = 3.0 * sum(int((s["bctype"][3:-3, 3:-3] == 0).sum()) * s["nsteps"] *
+                      (1330.0 if s["method"] == "weno" else 5300.0) for s in specs)
+    achieved = flops / (ms * 1e-3) / 1e12
+    cpu = {"value": None, "skipped": True}
+    if not args.no_cpu_baseline and world == 1:
+        r = batch_cpu_rates()
+        if r:
+            t_cpu = sum(int((s["bctype"][3:-3, 3:-3] == 0).sum()) * s["nsteps"] *
+                        (r["weno"] if s["method"] == "weno" else r["dg2"]) for s in specs)
+            cpu = {"value": rep["dof_updates"] / t_cpu, "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                   "sample": "per-cell-step cost of the reference's updateMesh measured on bounded strips "
+                             f"(WENO5: {r['weno_sample']}; DG P=2: {r['dg2_sample']}), applied to the batch's "
+                             "cell-steps", "cell_updates_per_s": rep["cell_updates"] / t_cpu}
+    lat = {p: {"p50_ms": v["rep"]["latency_p50_ms"], "p99_ms": v["rep"]["latency_p99_ms"],
+               "max_ms": v["rep"]["latency_max_ms"], "device_ms": v["rep"]["ms"],
+               "cell_updates_per_s": v["rep"]["cell_updates"] / (v["rep"]["ms"] * 1e-3),
+               "done": v["rep"]["done"], "failed": v["rep"]["failed"], "graph_launches": v["rep"]["graph_launches"]}
+           for p, v in results.items()}
+    out = {"metric": METRIC, "value": world * rep["dof_updates"] / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+           "steps": nsteps, "warmup": 3, "ms_per_step": ms / nsteps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+           "config": {"workload": args.workload, "problems": nprob, "steps_per_problem": nsteps,
+                      "desc": f"{nprob} seeded four-quadrant problems, sides uniform in {{128..1024 step 128}}, "
+                              "first half WENO5 (CFL 0.4), second half DG P=2 (0.5 x dgSafeDt, reference "
+                              "limiter), mixed precision, per-problem dt on the device; policy 'all'",
+                      "updated_cells": cells, "l2": "working set %.1f GB >> 126 MB L2" % (in_bytes * 2.5 / 1e9),
+                      "parallelism": f"replicas x{world}", "groups": head["groups"]},
+           "cell_updates_per_s": world * rep["cell_updates"] / (ms * 1e-3),
+           "latency": lat, "clocks": head["clocks"],
+           "e2e": {"value": world * rep["dof_updates"] / wall, "unit": UNIT,
+                   "h2d_bytes_per_step": in_bytes / nsteps, "d2h_bytes_per_step": in_bytes / nsteps,
+                   "what": "zk_batch_add of every problem from pinned host memory + zk_batch_run + "
+                           "zk_batch_get_state of every problem, host wall clock, policy 'all'"},
+           "gpu_launches": rep["kernel_launches"],
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                        "frac": achieved / peaks["fp32_tflops"], "traffic": None,
+                        "kernel": "whole batch run (all kernels of all groups)",
+                        "flops": "3 stages x cell-steps x (1330 WENO5, 5300 DG P=2)",
+                        "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU"},
+           "cpu_baseline": cpu, "peaks": peaks}
+    print(json.dumps(out), flush=True)
+
+
+def run_reference_batch(args) -> dict:
+    """The reference's CPU updateMesh over the batch's cell-steps, from its
+    per-cell-step cost on bounded strips (batch_cpu_rates)."""
+    from zuikakucfd_b200.batch import batch_sides
+    nprob, nsteps = parse_batch(args.workload)
+    r = batch_cpu_rates(4.0)
+    if not r:
+        return {"impl": "reference", "unavailable": "oracle/_ref (reference built from its sources) missing"}
+    sides = batch_sides(nprob, 1000)
+    half = nprob // 2
+    cells = [(s - 6) ** 2 for s in sides]
+    t = sum(c * nsteps * (r["weno"] if i < half else r["dg2"]) for i, c in enumerate(cells))
+    dofs = sum(c * nsteps * (4 if i < half else 36) for i, c in enumerate(cells))
+    v = dofs / t
+    return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": nsteps, "warmup": 0, "ms_per_step": t * 1e3 / nsteps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "problems": nprob},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": r["cores"], "kind": "reference",
+                             "sample": f"WENO5: {r['weno_sample']}; DG P=2: {r['dg2_sample']}; per-cell-step "
+                                       "costs applied to the batch's cell-steps"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def gpu_launches(w, prec) -> int:

@@ -183,6 +183,80 @@ int zk_weno_step_noalloc(double* state, int ny, int nx, int pitch, double da, do
                          const int32_t* bctype, double dt, int nsteps, void* stream,
                          uint32_t* status_out);
 
+/* ---- batched runner --------------------------------------------------------
+ * No counterpart in the reference, whose solver.cpp advances one mesh per
+ * process (src_WENO/solver.cpp:159-190, src_DG/solver.cpp:270-310).  A batch
+ * holds many independent problems of any sizes, WENO and DG mixed, each with
+ * its own step count and CFL number, and advances them on one GPU:
+ *   - problems with the same method, precision and order form a group; each RK
+ *     stage of a group is ONE persistent kernel launch over the tiles of all
+ *     its running problems (a device-side directory lists them);
+ *   - each step is max wave speed -> per-problem dt -> 3 stages -> step count,
+ *     all on the device (dt never goes through the host); graph_steps steps
+ *     of every group are captured once as a CUDA graph and replayed;
+ *   - an autotuner times the tile variants and persistent grid sizes of each
+ *     group's stage kernel before the first run;
+ *   - the scheduler admits all problems at once (ZK_BATCH_ALL) or
+ *     smallest-work-first while the running problems hold fewer than
+ *     active_cells updated cells (ZK_BATCH_SJF), refilling as problems finish.
+ * A problem's dt: WENO cfl*da/lambda (lambda = computeMaxSpeed of the step's
+ * input, src_WENO/fluid.cpp:539-553); DG cfl*dgSafeDt(lambda)
+ * (src_DG/solver.cpp:19-64).  DG limiters: REFERENCE or NONE. */
+typedef struct zk_batch zk_batch;
+
+enum { ZK_BATCH_ALL = 0, ZK_BATCH_SJF = 1 };
+enum { ZK_BATCH_WAITING = 0, ZK_BATCH_RUNNING = 1, ZK_BATCH_DONE = 2, ZK_BATCH_FAILED = 3 };
+
+typedef struct zk_batch_options {
+    int device;
+    int policy;           /* ZK_BATCH_*                                            */
+    double active_cells;  /* SJF admission bound in updated cells (<= 0: 8e6)      */
+    int graph_steps;      /* RK steps per captured graph (1..1000; default 10)     */
+    int autotune;         /* 0 off, 1 on (cached per process), 2 re-tune           */
+    size_t arena_bytes;   /* > 0: one device allocation all problems carve from    */
+} zk_batch_options;
+
+typedef struct zk_batch_report {
+    double ms;              /* device time of the run (CUDA events)               */
+    double cell_updates;    /* sum over problems of updated cells x steps taken   */
+    double dof_updates;     /* the same x DOF per cell (4, or 4 (P+1)^2 for DG)   */
+    double latency_p50_ms;  /* per-problem completion time from the run's start   */
+    double latency_p99_ms;
+    double latency_max_ms;
+    int problems, done, failed;
+    int graph_launches, graph_steps;
+    long long kernel_launches; /* kernels the replayed graphs launched            */
+} zk_batch_report;
+
+typedef struct zk_batch_problem {
+    int state;          /* ZK_BATCH_*                                  */
+    int steps_done;
+    double t;           /* simulated time reached                      */
+    double latency_ms;  /* completion time from the run's start, or -1 */
+    uint32_t status;    /* status word bits of this problem's kernels  */
+    int group;
+} zk_batch_problem;
+
+void zk_batch_default_options(zk_batch_options* o);
+int zk_batch_create(const zk_batch_options* o, zk_batch** out);
+/* Register one problem: options as for zk_create, mesh as for zk_set_mesh,
+ * initial state as for zk_set_state (host layout above).  *id = 0, 1, ... */
+int zk_batch_add(zk_batch* b, const zk_options* opt, int ny, int nx, double da, double gamma,
+                 const int32_t* bctype, const double* state, int nsteps, double cfl, int* id);
+/* Advance every problem to its step count (once per batch). */
+int zk_batch_run(zk_batch* b, zk_batch_report* report);
+int zk_batch_get_state(zk_batch* b, int id, double* host);
+int zk_batch_problem_info(zk_batch* b, int id, zk_batch_problem* out);
+/* The dt of each step problem `id` took (n <= its step count). */
+int zk_batch_dt_history(zk_batch* b, int id, double* dts, int n);
+/* Chosen configuration of group g (groups form at zk_batch_run): tile variant
+ * (index into the tile heights {4, 8} for WENO, {2, 4} for mixed DG) and CTAs
+ * per SM of the stage kernel; *ngroups = number of groups.  Any pointer may be
+ * NULL; g = -1 only reports the number of groups. */
+int zk_batch_group_config(zk_batch* b, int g, int* method, int* precision, int* order, int* variant,
+                          int* ctas_per_sm, int* ngroups);
+void zk_batch_destroy(zk_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

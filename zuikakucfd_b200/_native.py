@@ -38,6 +38,27 @@ class zk_options(C.Structure):
                 ("device", C.c_int), ("tvb_M", C.c_double)]
 
 
+class zk_batch_options(C.Structure):
+    _fields_ = [("device", C.c_int), ("policy", C.c_int), ("active_cells", C.c_double),
+                ("graph_steps", C.c_int), ("autotune", C.c_int), ("arena_bytes", C.c_size_t)]
+
+
+class zk_batch_report(C.Structure):
+    _fields_ = [("ms", C.c_double), ("cell_updates", C.c_double), ("dof_updates", C.c_double),
+                ("latency_p50_ms", C.c_double), ("latency_p99_ms", C.c_double),
+                ("latency_max_ms", C.c_double), ("problems", C.c_int), ("done", C.c_int),
+                ("failed", C.c_int), ("graph_launches", C.c_int), ("graph_steps", C.c_int),
+                ("kernel_launches", C.c_longlong)]
+
+
+class zk_batch_problem(C.Structure):
+    _fields_ = [("state", C.c_int), ("steps_done", C.c_int), ("t", C.c_double),
+                ("latency_ms", C.c_double), ("status", C.c_uint32), ("group", C.c_int)]
+
+
+POLICY = {"all": 0, "sjf": 1}
+BATCH_STATE = {0: "waiting", 1: "running", 2: "done", 3: "failed"}
+
 _lock = threading.Lock()
 _lib: C.CDLL | None = None
 
@@ -79,6 +100,16 @@ _SIGS = {
     "zk_weno_step_noalloc": (C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int32), C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_uint32)]),
+    "zk_batch_default_options": (None, [C.POINTER(zk_batch_options)]),
+    "zk_batch_create": (C.c_int, [C.POINTER(zk_batch_options), C.POINTER(_P)]),
+    "zk_batch_add": (C.c_int, [_P, C.POINTER(zk_options), C.c_int, C.c_int, C.c_double, C.c_double,
+                               C.POINTER(C.c_int32), _D, C.c_int, C.c_double, C.POINTER(C.c_int)]),
+    "zk_batch_run": (C.c_int, [_P, C.POINTER(zk_batch_report)]),
+    "zk_batch_get_state": (C.c_int, [_P, C.c_int, _D]),
+    "zk_batch_problem_info": (C.c_int, [_P, C.c_int, C.POINTER(zk_batch_problem)]),
+    "zk_batch_dt_history": (C.c_int, [_P, C.c_int, _D, C.c_int]),
+    "zk_batch_group_config": (C.c_int, [_P, C.c_int] + [C.POINTER(C.c_int)] * 6),
+    "zk_batch_destroy": (None, [_P]),
 }
 
 

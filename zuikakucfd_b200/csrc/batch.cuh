@@ -1,0 +1,103 @@
+// Device-side structures of the batched runner: many independent problems of
+// uneven grid sizes advanced together by persistent kernels.
+//
+// Every problem owns a control block (BatchCtl) that the per-step control
+// kernels update on the device: the time step from the problem's own CFL
+// rule, the step counter, the done/failed state and the completion time.
+// A problem group (problems sharing method, precision and order) owns one
+// item array (per-problem pointers and sizes) and, per tiling, a directory:
+//
+//   dir[0] = n (problems listed), dir[1] = total tiles,
+//   dir[2 .. 2+cap)        = item index of each listed problem,
+//   dir[2+cap .. 2+2cap)   = exclusive end of each problem's tile range.
+//
+// The host rewrites directories between graph launches (admission), so the
+// captured kernels stay valid while the set of running problems changes.
+#pragma once
+
+#include <cuda.h>
+#include <cstdint>
+#include "zk_common.cuh"
+
+namespace zk {
+
+enum : int { BATCH_WAITING = 0, BATCH_RUNNING = 1, BATCH_DONE = 2, BATCH_FAILED = 3 };
+
+struct BatchCtl {
+    double dt, dtdx, dtdy;      // time step of the current step, and dt/da
+    double t;                   // simulated time reached
+    double cfl;                 // CFL number of the problem's dt rule
+    double da;
+    unsigned long long lam;     // max wave speed of the step's input (double bits, atomicMax)
+    unsigned long long t_done;  // %globaltimer (ns) when the problem finished or failed
+    double* dtlog;              // dt of every step taken, [steps_target]
+    int steps_done, steps_target;
+    int state;                  // BATCH_*
+    int stepping;               // 1 while the current step advances this problem
+    int method, order;
+    uint32_t status;            // STATUS_* bits of this problem's kernels
+    int pad;
+};
+
+// Tile heights of the WENO stage kernels the autotuner chooses between.
+constexpr int kWenoTileRows[2] = {4, 8};
+// Tile heights of the mixed-precision DG stage kernel.
+constexpr int kDgTileRows[2] = {2, 4};
+
+// One WENO problem of a group.  tmap[v][b]: TMA map over buffer b (U^n,
+// stage 1, stage 2) with the box of tile variant v (mixed precision only).
+struct alignas(64) WenoItem {
+    CUtensorMap tmap[2][3];
+    double* U[3];
+    const int8_t* kind;
+    const int32_t* gsrc;
+    BatchCtl* ctl;
+    Grid g;
+    double gamma;
+};
+
+// One DG problem of a group.
+struct DgItem {
+    double* U[3];       // U^n and the two FP64 stage states (FP64 path)
+    float* F[2];        // FP32 stage states (mixed path)
+    double* fx;         // face fluxes (FP64 path)
+    double* fy;
+    const int8_t* kind;
+    const int32_t* gsrc;
+    const double* phic;  // basis at the 4 cell corners [NM][4] (CFL reduction)
+    BatchCtl* ctl;
+    Grid g;
+    int xpitch, nm;
+    double inv2h, gamma, s0;
+    int limiter, hll;
+};
+
+// Index of the listed problem whose tile range holds global tile t.
+__device__ __forceinline__ int dir_find(const int* __restrict__ end, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(end + mid) > t) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// The problem (item index) and problem-local tile of global tile t.
+struct DirHit {
+    int item, local;
+};
+__device__ __forceinline__ DirHit dir_lookup(const int* __restrict__ dir, int cap, int t) {
+    const int n = __ldg(dir);
+    const int* end = dir + 2 + cap;
+    const int s = dir_find(end, n, t);
+    return {__ldg(dir + 2 + s), t - (s ? __ldg(end + s - 1) : 0)};
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+}  // namespace zk

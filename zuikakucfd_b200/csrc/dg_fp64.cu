@@ -20,6 +20,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "batch.cuh"
 #include "dg_common.cuh"
 #include "zk_internal.h"
 
@@ -248,12 +249,13 @@ __device__ __forceinline__ void cell_traces(const DGArgs& a, CellRef r, const do
 
 // One thread per interface.  DIR 0: x face (i, jf) between cells (i, jf-1)
 // and (i, jf); DIR 1: y face (if, j) between (if-1, j) above and (if, j) below.
+// Faces (i, jb + threadIdx.x).
 template <int P, int DIR>
-__global__ void __launch_bounds__(128) dg_face_kernel(DGArgs a) {
+__device__ __forceinline__ void face_row(const DGArgs& a, int jb, int i) {
     constexpr int NQ = P + 1;
     const DGTab& T = c_dgtab[P - 1];
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x, i = blockIdx.y;
+    const int j = jb + threadIdx.x;
     size_t kl, kr;  // the two cells
     if (DIR == 0) {
         if (j < 1 || j >= nx || i >= ny) return;
@@ -289,6 +291,11 @@ __global__ void __launch_bounds__(128) dg_face_kernel(DGArgs a) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) F[(size_t)(q * 4 + c) * qstride + o] = f[c];
     }
+}
+
+template <int P, int DIR>
+__global__ void __launch_bounds__(128) dg_face_kernel(DGArgs a) {
+    face_row<P, DIR>(a, blockIdx.x * blockDim.x, blockIdx.y);
 }
 
 // applyLimiter for one cell held in registers (src_DG/fluid.cpp:824-992):
@@ -378,13 +385,15 @@ __device__ __forceinline__ void limit_cell(double (&o)[4][(P + 1) * (P + 1)], bo
 
 constexpr int kCellBlock = 64;
 
+// Cells (i, jb + threadIdx.x); sd[v][threadIdx.x] is this thread's (filled)
+// stage input, column-private.
 template <int P>
-__global__ void __launch_bounds__(kCellBlock) dg_cell_kernel(DGArgs a) {
+__device__ __forceinline__ void cell_row(const DGArgs& a, int jb, int i,
+                                         double (&sd)[4 * (P + 1) * (P + 1)][kCellBlock]) {
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
     const DGTab& T = c_dgtab[P - 1];
-    __shared__ double sd[4 * NM][kCellBlock];  // this thread's (filled) stage input, column-private
     const int t = threadIdx.x;
-    const int j = blockIdx.x * kCellBlock + t, i = blockIdx.y;
+    const int j = jb + t;
     if (j >= a.g.nx) return;  // no block-wide synchronisation follows
     const int ny = a.g.ny, nx = a.g.nx;
     const size_t plane = a.g.plane, k = (size_t)i * a.g.pitch + j;
@@ -488,6 +497,94 @@ __global__ void __launch_bounds__(kCellBlock) dg_cell_kernel(DGArgs a) {
     for (int v = 0; v < 4 * NM; ++v) a.out[(size_t)v * plane + k] = o[v / NM][v % NM];
 }
 
+template <int P>
+__global__ void __launch_bounds__(kCellBlock) dg_cell_kernel(DGArgs a) {
+    __shared__ double sd[4 * (P + 1) * (P + 1)][kCellBlock];
+    cell_row<P>(a, blockIdx.x * kCellBlock, blockIdx.y, sd);
+}
+
+// Stage-s arguments of batch item `it` (stage s reads U[s-1], writes U[s % 3]).
+__device__ __forceinline__ DGArgs batch_args(const DgItem& it, int stage) {
+    const BatchCtl* ctl = it.ctl;
+    DGArgs a;
+    a.cur = it.U[stage - 1];
+    a.un = it.U[0];
+    a.out = it.U[stage % 3];
+    a.kind = it.kind;
+    a.gsrc = it.gsrc;
+    a.fx = it.fx;
+    a.fy = it.fy;
+    a.g = it.g;
+    a.xpitch = it.xpitch;
+    a.dt = ctl->dt;
+    a.inv2h = it.inv2h;
+    a.gamma = it.gamma;
+    a.stage = stage;
+    a.limiter = it.limiter;
+    a.hll = it.hll;
+    a.s0 = it.s0;
+    a.status = &it.ctl->status;
+    return a;
+}
+
+// Persistent face pass of a batch group: a problem's tiles are its x-face
+// rows (ny x ceil(nx/128) segments) followed by its y-face rows.
+template <int P>
+__global__ void __launch_bounds__(128) dg_faces_fp64_batch_kernel(const DgItem* __restrict__ items,
+                                                                   const int* __restrict__ dir, int cap, int stage) {
+    __shared__ DGArgs sa;
+    __shared__ int s_job[4];  // stepping, direction, row, segment start
+    const int total = __ldg(dir + 1);
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const DirHit h = dir_lookup(dir, cap, t);
+            const DgItem& it = items[h.item];
+            s_job[0] = it.ctl->stepping;
+            if (s_job[0]) {
+                const int segs = (it.g.nx + 127) / 128, per = it.g.ny * segs;
+                const int d = h.local >= per, r = h.local - d * per;
+                s_job[1] = d;
+                s_job[2] = r / segs;
+                s_job[3] = (r - (r / segs) * segs) * 128;
+                sa = batch_args(it, stage);
+            }
+        }
+        __syncthreads();
+        if (s_job[0]) {
+            if (s_job[1] == 0) face_row<P, 0>(sa, s_job[3], s_job[2]);
+            else face_row<P, 1>(sa, s_job[3], s_job[2]);
+        }
+        __syncthreads();
+    }
+}
+
+// Persistent cell pass of a batch group: tiles are row segments of kCellBlock cells.
+template <int P>
+__global__ void __launch_bounds__(kCellBlock) dg_cell_fp64_batch_kernel(const DgItem* __restrict__ items,
+                                                                         const int* __restrict__ dir, int cap,
+                                                                         int stage) {
+    __shared__ double sd[4 * (P + 1) * (P + 1)][kCellBlock];
+    __shared__ DGArgs sa;
+    __shared__ int s_job[3];  // stepping, row, segment start
+    const int total = __ldg(dir + 1);
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const DirHit h = dir_lookup(dir, cap, t);
+            const DgItem& it = items[h.item];
+            s_job[0] = it.ctl->stepping;
+            if (s_job[0]) {
+                const int segs = (it.g.nx + kCellBlock - 1) / kCellBlock;
+                s_job[1] = h.local / segs;
+                s_job[2] = (h.local - s_job[1] * segs) * kCellBlock;
+                sa = batch_args(it, stage);
+            }
+        }
+        __syncthreads();
+        if (s_job[0]) cell_row<P>(sa, s_job[2], s_job[1], sd);
+        __syncthreads();
+    }
+}
+
 // applyLimiter alone, in place on the state (src_DG/fluid.cpp:824-992).
 template <int P>
 __global__ void __launch_bounds__(kCellBlock) dg_limit_kernel(DGArgs a) {
@@ -528,6 +625,45 @@ cudaError_t launch_dg_stage_fp64(int P, const DGArgs& a, cudaStream_t s) {
         case 3: return launch_stage<3>(a, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// Batch tiles per problem: face pass 2 ny ceil(nx/128), cell pass ny ceil(nx/64).
+int dg_fp64_batch_tiles(int pass, int ny, int nx) {
+    return pass == 0 ? 2 * ny * ((nx + 127) / 128) : ny * ((nx + kCellBlock - 1) / kCellBlock);
+}
+
+template <int P>
+cudaError_t launch_batch_p(const DgItem* items, const int* dir_face, const int* dir_cell, int cap, int stage,
+                           int grid_face, int grid_cell, cudaStream_t s) {
+    dg_faces_fp64_batch_kernel<P><<<grid_face, 128, 0, s>>>(items, dir_face, cap, stage);
+    dg_cell_fp64_batch_kernel<P><<<grid_cell, kCellBlock, 0, s>>>(items, dir_cell, cap, stage);
+    return cudaGetLastError();
+}
+
+// One FP64 DG stage of a batch group (face pass, then cell pass).
+cudaError_t launch_dg_stage_fp64_batch(int P, const DgItem* items, const int* dir_face, const int* dir_cell, int cap,
+                                       int stage, int grid_face, int grid_cell, cudaStream_t s) {
+    switch (P) {
+        case 1: return launch_batch_p<1>(items, dir_face, dir_cell, cap, stage, grid_face, grid_cell, s);
+        case 2: return launch_batch_p<2>(items, dir_face, dir_cell, cap, stage, grid_face, grid_cell, s);
+        case 3: return launch_batch_p<3>(items, dir_face, dir_cell, cap, stage, grid_face, grid_cell, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Resident CTAs per SM of the batch face (pass 0) and cell (pass 1) kernels.
+int dg_fp64_batch_occupancy(int P, int pass) {
+    int n = 0;
+    switch (P * 2 + pass) {
+        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_faces_fp64_batch_kernel<1>, 128, 0); break;
+        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_cell_fp64_batch_kernel<1>, kCellBlock, 0); break;
+        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_faces_fp64_batch_kernel<2>, 128, 0); break;
+        case 5: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_cell_fp64_batch_kernel<2>, kCellBlock, 0); break;
+        case 6: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_faces_fp64_batch_kernel<3>, 128, 0); break;
+        case 7: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, dg_cell_fp64_batch_kernel<3>, kCellBlock, 0); break;
+        default: break;
+    }
+    return n;
 }
 
 cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s) {

@@ -14,6 +14,9 @@
 #include <cstring>
 #include <mutex>
 
+#include <type_traits>
+
+#include "batch.cuh"
 #include "dg_common.cuh"
 #include "zk_internal.h"
 
@@ -32,8 +35,9 @@ struct DGTabF {
 
 __constant__ DGTabF c_tabf[3];
 
-constexpr int MTX = 32, MTY = 4, MNT = MTX * MTY;
-constexpr int SX = MTX + 2, SY = MTY + 2;  // tile + 1-cell halo
+// A tile is 32 x MTY cells with one thread per cell; shared memory holds the
+// tile plus a 1-cell halo (SX x (MTY + 2) slots).
+constexpr int MTX = 32, SX = MTX + 2;
 
 struct MixArgs {
     const void* cur;  // stage input: double (stage 1: U^n) or float (U^(1), U^(2))
@@ -144,20 +148,22 @@ __device__ __forceinline__ float load_f(const void* p, size_t i) {
     return (float)static_cast<const T*>(p)[i];
 }
 
-template <int P, typename TIn, typename TOut>
-__global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
+// One tile whose top-left cell is (i0, j0), shared memory at `smem`
+// (smem_bytes<P, MTY>()).  Per-thread returns leave only this function: every
+// barrier of the tile precedes them.
+template <int P, typename TIn, typename TOut, int MTY>
+__device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
+    constexpr int MNT = MTX * MTY, SY = MTY + 2;
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
     constexpr int SD = SX * SY;  // cell slots of the tile + halo
     constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
     const DGTabF& T = c_tabf[P - 1];
-    extern __shared__ __align__(16) float smem[];
     float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
     float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
     float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
     uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
 
     const int tid = threadIdx.x;
-    const int j0 = blockIdx.x * MTX, i0 = blockIdx.y * MTY;
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
 
@@ -484,15 +490,92 @@ __global__ void __launch_bounds__(MNT, 3) dg_stage_mixed_kernel(MixArgs a) {
     if (flags) atomicOr(a.status, flags);
 }
 
-template <int P>
+template <int P, int MTY>
 constexpr size_t smem_bytes() {
-    constexpr int NQ = P + 1, NM = NQ * NQ;
+    constexpr int NQ = P + 1, NM = NQ * NQ, SY = MTY + 2;
     return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
 }
 
 template <int P, typename TIn, typename TOut>
+__global__ void __launch_bounds__(MTX * 4, 3) dg_stage_mixed_kernel(MixArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    stage_tile<P, TIn, TOut, 4>(a, blockIdx.x * MTX, blockIdx.y * 4, smem);
+}
+
+// Persistent stage STAGE over every listed problem of a batch group, tile
+// variant V (kDgTileRows[V] rows): stage 1 reads U^n (FP64) and writes F[0],
+// stage 2 reads F[0] and writes F[1], stage 3 reads F[1] and writes U^n.
+template <int P, int STAGE, int V>
+__global__ void __launch_bounds__(MTX * kDgTileRows[V], 12 / kDgTileRows[V])
+    dg_stage_mixed_batch_kernel(const DgItem* __restrict__ items, const int* __restrict__ dir, int cap) {
+    constexpr int MTY = kDgTileRows[V];
+    using TIn = typename std::conditional<STAGE == 1, double, float>::type;
+    using TOut = typename std::conditional<STAGE == 3, double, float>::type;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ MixArgs sa;  // the current tile's problem, kept out of registers
+    __shared__ int s_org[3];
+    const int total = __ldg(dir + 1);
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const DirHit h = dir_lookup(dir, cap, t);
+            const DgItem& it = items[h.item];
+            BatchCtl* ctl = it.ctl;
+            s_org[2] = ctl->stepping;
+            if (s_org[2]) {
+                const int tiles_x = (it.g.nx + MTX - 1) / MTX;
+                const int ty = h.local / tiles_x;
+                s_org[0] = (h.local - ty * tiles_x) * MTX;
+                s_org[1] = ty * MTY;
+                const void* cur = STAGE == 1 ? (const void*)it.U[0] : (const void*)it.F[STAGE - 2];
+                void* out = STAGE == 3 ? (void*)it.U[0] : (void*)it.F[STAGE - 1];
+                sa = MixArgs{cur, it.U[0], out, it.kind, it.gsrc, it.g, ctl->dt, (float)it.inv2h, (float)it.gamma,
+                             STAGE, it.limiter, it.hll, (float)it.s0, &ctl->status};
+            }
+        }
+        __syncthreads();
+        if (s_org[2]) stage_tile<P, TIn, TOut, MTY>(sa, s_org[0], s_org[1], smem);
+        __syncthreads();
+    }
+}
+
+template <int P, int STAGE, int V>
+cudaError_t batch_one(const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s, int* occ) {
+    constexpr size_t sm = smem_bytes<P, kDgTileRows[V]>();
+    constexpr int nt = MTX * kDgTileRows[V];
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(dg_stage_mixed_batch_kernel<P, STAGE, V>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+        attr_set[dev] = true;
+    }
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, dg_stage_mixed_batch_kernel<P, STAGE, V>, nt, sm);
+    dg_stage_mixed_batch_kernel<P, STAGE, V><<<grid, nt, sm, s>>>(items, dir, cap);
+    return cudaGetLastError();
+}
+
+template <int P, int V>
+cudaError_t batch_pv(int stage, const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s, int* occ) {
+    switch (stage) {
+        case 1: return batch_one<P, 1, V>(items, dir, cap, grid, s, occ);
+        case 2: return batch_one<P, 2, V>(items, dir, cap, grid, s, occ);
+        case 3: return batch_one<P, 3, V>(items, dir, cap, grid, s, occ);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int P>
+cudaError_t batch_p(int variant, int stage, const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s,
+                    int* occ) {
+    return variant == 0 ? batch_pv<P, 0>(stage, items, dir, cap, grid, s, occ)
+                        : batch_pv<P, 1>(stage, items, dir, cap, grid, s, occ);
+}
+
+template <int P, typename TIn, typename TOut>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
-    constexpr size_t sm = smem_bytes<P>();
+    constexpr size_t sm = smem_bytes<P, 4>();
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -502,8 +585,8 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
-    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + MTY - 1) / MTY);
-    dg_stage_mixed_kernel<P, TIn, TOut><<<grid, MNT, sm, s>>>(a);
+    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + 3) / 4);
+    dg_stage_mixed_kernel<P, TIn, TOut><<<grid, MTX * 4, sm, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -537,6 +620,35 @@ int dg_upload_tables_f32(int P) {
     if (cudaMemcpyToSymbol(c_tabf, &F, sizeof F, sizeof F * (P - 1)) != cudaSuccess) return ZK_ERR_CUDA;
     done[dev] |= (1ull << P);
     return ZK_OK;
+}
+
+// One mixed-precision DG stage of a batch group (grid persistent CTAs).
+cudaError_t launch_dg_stage_mixed_batch(int P, int variant, int stage, const DgItem* items, const int* dir, int cap,
+                                        int grid, cudaStream_t s) {
+    switch (P) {
+        case 1: return batch_p<1>(variant, stage, items, dir, cap, grid, s, nullptr);
+        case 2: return batch_p<2>(variant, stage, items, dir, cap, grid, s, nullptr);
+        case 3: return batch_p<3>(variant, stage, items, dir, cap, grid, s, nullptr);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// Resident CTAs per SM of the batch stage kernel (0 on error).
+int dg_mixed_batch_occupancy(int P, int variant, int stage) {
+    int n = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (P) {
+        case 1: e = batch_p<1>(variant, stage, nullptr, nullptr, 0, 0, nullptr, &n); break;
+        case 2: e = batch_p<2>(variant, stage, nullptr, nullptr, 0, 0, nullptr, &n); break;
+        case 3: e = batch_p<3>(variant, stage, nullptr, nullptr, 0, 0, nullptr, &n); break;
+        default: break;
+    }
+    return e == cudaSuccess ? n : 0;
+}
+
+// Tiles of one problem for tile variant v.
+int dg_mixed_batch_tiles(int variant, int ny, int nx) {
+    return ((nx + MTX - 1) / MTX) * ((ny + kDgTileRows[variant] - 1) / kDgTileRows[variant]);
 }
 
 // One mixed-precision DG stage: cur (double if in_fp64 else float) -> out

@@ -12,15 +12,20 @@
 // evaluations see the same six inputs in the same order and give the same
 // bits), then forms dU and the Shu-Osher combine for every cell of the tile,
 // ghosts included, exactly as the reference's whole-array Eigen expressions do.
+#include "batch.cuh"
 #include "zk_common.cuh"
 #include "zk_kernels.h"
 
 namespace zk {
 namespace {
 
-constexpr int TX = 32, TY = 8, HX = TX + 6, HY = TY + 6;
-constexpr int NWARP = 9;  // 18 warp tasks (8+1 x-face rows, 9 y-face rows) in 2 rounds
-constexpr int NTHREAD = NWARP * 32;
+// A tile is 32 x TY cells; TY + 1 warps take the 2 TY + 2 face-row tasks
+// (TY + 1 x-face rows, TY + 1 y-face rows) in two rounds.
+constexpr int TX = 32, HX = TX + 6;
+template <int TY>
+struct Tile {
+    static constexpr int HY = TY + 6, NWARP = TY + 1, NTHREAD = NWARP * 32;
+};
 
 // weno5_reconstruct, src_WENO/fluid.cpp:230-263
 __device__ __forceinline__ void weno5(double UL2, double UL1, double UP, double UR1, double UR2,
@@ -108,13 +113,23 @@ struct StageArgs {
     uint32_t* status;
 };
 
-__global__ void __launch_bounds__(NTHREAD, 2) weno_stage_fp64_kernel(StageArgs a) {
-    __shared__ double sU[4][HY][HX];
-    __shared__ double sFx[4][TY][TX + 1];
-    __shared__ double sFy[4][TY + 1][TX];
-    __shared__ int8_t sK[HY][HX];
+template <int TY>
+struct Smem {
+    double sU[4][TY + 6][HX];
+    double sFx[4][TY][TX + 1];
+    double sFy[4][TY + 1][TX];
+    int8_t sK[TY + 6][HX];
+};
 
-    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TY;
+// One tile whose top-left cell is (i0, j0).  Ends with every thread past its
+// last shared-memory read, so a persistent caller may reuse S after a barrier.
+template <int TY>
+__device__ __forceinline__ void stage_tile(const StageArgs& a, int j0, int i0, Smem<TY>& S) {
+    constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
+    auto& sU = S.sU;
+    auto& sFx = S.sFx;
+    auto& sFy = S.sFy;
+    auto& sK = S.sK;
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
 
@@ -215,15 +230,72 @@ __global__ void __launch_bounds__(NTHREAD, 2) weno_stage_fp64_kernel(StageArgs a
     if (flags && lane == 0) atomicOr(a.status, flags);
 }
 
+__global__ void __launch_bounds__(Tile<8>::NTHREAD, 2) weno_stage_fp64_kernel(StageArgs a) {
+    __shared__ Smem<8> S;
+    stage_tile<8>(a, blockIdx.x * TX, blockIdx.y * 8, S);
+}
+
+// Persistent stage over every listed problem of a batch group: CTA b takes
+// global tiles b, b + gridDim.x, ...; stage s reads U[s-1] (U^n at stage 1)
+// and writes U[s % 3].
+template <int TY>
+__global__ void __launch_bounds__(Tile<TY>::NTHREAD, 16 / (TY + 1) + 1)
+    weno_stage_fp64_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
+                                 int stage) {
+    __shared__ Smem<TY> S;
+    __shared__ StageArgs sa;  // the current tile's problem, kept out of registers
+    __shared__ int s_org[3];  // tile origin x, y; 0 when the problem is not stepping
+    const int total = __ldg(dir + 1);
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const DirHit h = dir_lookup(dir, cap, t);
+            const WenoItem& it = items[h.item];
+            BatchCtl* ctl = it.ctl;
+            s_org[2] = ctl->stepping;
+            if (s_org[2]) {
+                const int tiles_x = (it.g.nx + TX - 1) / TX;
+                const int ty = h.local / tiles_x;
+                s_org[0] = (h.local - ty * tiles_x) * TX;
+                s_org[1] = ty * TY;
+                sa = StageArgs{it.U[stage - 1], it.U[0], it.U[stage % 3], it.kind, it.gsrc, it.g,
+                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status};
+            }
+        }
+        __syncthreads();
+        if (s_org[2]) stage_tile<TY>(sa, s_org[0], s_org[1], S);
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_weno_stage_fp64_batch(int variant, const WenoItem* items, const int* dir, int cap, int stage,
+                                         int grid, cudaStream_t s) {
+    if (variant == 0)
+        weno_stage_fp64_batch_kernel<kWenoTileRows[0]><<<grid, Tile<kWenoTileRows[0]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
+    else
+        weno_stage_fp64_batch_kernel<kWenoTileRows[1]><<<grid, Tile<kWenoTileRows[1]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
+    return cudaGetLastError();
+}
+
+int weno_fp64_batch_occupancy(int variant) {
+    int n = 0;
+    if (variant == 0)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_fp64_batch_kernel<kWenoTileRows[0]>,
+                                                      Tile<kWenoTileRows[0]>::NTHREAD, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_fp64_batch_kernel<kWenoTileRows[1]>,
+                                                      Tile<kWenoTileRows[1]>::NTHREAD, 0);
+    return n;
+}
 
 cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
                                    const int8_t* kind, const int32_t* gsrc, const Grid& g,
                                    double dtdx, double dtdy, double gamma, int stage,
                                    uint32_t* status, cudaStream_t s) {
     StageArgs a{Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status};
-    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY);
-    weno_stage_fp64_kernel<<<grid, NTHREAD, 0, s>>>(a);
+    dim3 grid((g.nx + TX - 1) / TX, (g.ny + 7) / 8);
+    weno_stage_fp64_kernel<<<grid, Tile<8>::NTHREAD, 0, s>>>(a);
     return cudaGetLastError();
 }
 

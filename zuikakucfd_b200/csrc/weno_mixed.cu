@@ -15,6 +15,7 @@
 // brings the CTA's 40 x 14 x 4 FP64 box (tile + 3-cell halo, x start rounded
 // down to a 16-byte boundary) into shared memory; the completion wait is
 // bounded and reports STATUS_TIMEOUT instead of hanging.
+#include "batch.cuh"
 #include "tma.cuh"
 #include "tma_host.h"
 #include "zk_common.cuh"
@@ -23,10 +24,13 @@
 namespace zk {
 namespace {
 
-constexpr int TX = 32, TY = 8, HX = TX + 6, HY = TY + 6;
+// A tile is 32 x TY cells; TY + 1 warps take the 2 TY + 2 face-row tasks.
+constexpr int TX = 32, HX = TX + 6;
 constexpr int SX = TX + 8;  // staged columns: x from j0-4 (16-byte aligned) to j0+35
-constexpr int NWARP = 9;
-constexpr int NTHREAD = NWARP * 32;
+template <int TY>
+struct Tile {
+    static constexpr int HY = TY + 6, NWARP = TY + 1, NTHREAD = NWARP * 32;
+};
 constexpr uint8_t HIGH_MACH = 0x10;
 
 // weno5_reconstruct (src_WENO/fluid.cpp:230-263), any precision.
@@ -125,35 +129,44 @@ struct MixedArgs {
     uint32_t* status;
 };
 
-__global__ void __launch_bounds__(NTHREAD, 3)
-    weno_stage_mixed_kernel(const __grid_constant__ CUtensorMap tmap, MixedArgs a) {
-    __shared__ __align__(128) double stg[4][HY][SX];  // TMA destination, FP64, ghosts fixed up in place
-    __shared__ float sU[4][HY][HX];                   // FP32 copy of the tile + halo
-    __shared__ double sFx[4][TY][TX + 1];
-    __shared__ double sFy[4][TY + 1][TX];
-    __shared__ uint8_t sK[HY][HX];                    // kind | HIGH_MACH
-    __shared__ __align__(8) uint64_t bar;
+template <int TY>
+struct Smem {
+    double stg[4][TY + 6][SX];  // TMA destination, FP64, ghosts fixed up in place (offset 0: 128-byte aligned)
+    float sU[4][TY + 6][HX];    // FP32 copy of the tile + halo
+    double sFx[4][TY][TX + 1];
+    double sFy[4][TY + 1][TX];
+    uint8_t sK[TY + 6][HX];     // kind | HIGH_MACH
+};
 
-    const int j0 = blockIdx.x * TX, i0 = blockIdx.y * TY;
+// One tile whose top-left cell is (i0, j0); `bar` is an initialised mbarrier
+// whose current phase has parity `phase`.  Returns false (after recording
+// STATUS_TIMEOUT) when the TMA copy did not land within the spin limit.
+// Every thread is past its last shared-memory access on return.
+template <int TY>
+__device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedArgs& a, int j0, int i0, Smem<TY>& S,
+                                           uint64_t* bar, uint32_t phase) {
+    constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
+    auto& stg = S.stg;
+    auto& sU = S.sU;
+    auto& sFx = S.sFx;
+    auto& sFy = S.sFy;
+    auto& sK = S.sK;
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
 
-    // 1. TMA: the 40 x 14 x 4 box starting at (j0-4, i0-3, 0); out-of-range
+    // 1. TMA: the 40 x (TY+6) x 4 box starting at (j0-4, i0-3, 0); out-of-range
     //    elements arrive as zeros
     if (threadIdx.x == 0) {
-        tma_prefetch_desc(&tmap);
-        mbar_init(&bar, 1);
-        mbar_arrive_expect_tx(&bar, (uint32_t)sizeof(stg));
-        tma_load_3d(&stg[0][0][0], &tmap, &bar, j0 - 4, i0 - 3, 0);
+        mbar_arrive_expect_tx(bar, (uint32_t)sizeof(stg));
+        tma_load_3d(&stg[0][0][0], tmap, bar, j0 - 4, i0 - 3, 0);
     }
-    __syncthreads();
-    const bool ok = mbar_wait_bounded(&bar, 0);
+    const bool ok = mbar_wait_bounded(bar, phase);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) {
             atomicOr(a.status, STATUS_TIMEOUT);
-            mbar_wait_bounded(&bar, 0);  // give a late copy a second bounded chance to land
+            mbar_wait_bounded(bar, phase);  // give a late copy a second bounded chance to land
         }
-        return;
+        return false;
     }
 
     // 2. ghost fill from the source map, FP32 copy, high-Mach flags
@@ -280,25 +293,104 @@ __global__ void __launch_bounds__(NTHREAD, 3)
     }
     flags = __reduce_or_sync(0xffffffffu, flags);
     if (flags && lane == 0) atomicOr(a.status, flags);
+    // the next TMA copy overwrites stg, which this tile wrote through the generic proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    return true;
+}
+
+__global__ void __launch_bounds__(Tile<8>::NTHREAD, 3)
+    weno_stage_mixed_kernel(const __grid_constant__ CUtensorMap tmap, MixedArgs a) {
+    __shared__ __align__(128) Smem<8> S;
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        tma_prefetch_desc(&tmap);
+        mbar_init(&bar, 1);
+    }
+    __syncthreads();
+    stage_tile<8>(&tmap, a, blockIdx.x * TX, blockIdx.y * 8, S, &bar, 0);
+}
+
+// Persistent stage over every listed problem of a batch group (tile variant
+// v: kWenoTileRows[v] rows).  The tensor maps live in the item array in
+// global memory, written by the host before the launch.
+template <int V>
+__global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 24 / (kWenoTileRows[V] + 1) + 1)
+    weno_stage_mixed_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
+                                  int stage) {
+    constexpr int TY = kWenoTileRows[V];
+    __shared__ __align__(128) Smem<TY> S;
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ MixedArgs sa;  // the current tile's problem, kept out of registers
+    __shared__ int s_org[3];  // tile origin x, y; 0 when the problem is not stepping
+    __shared__ const CUtensorMap* s_map;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    const int total = __ldg(dir + 1);
+    uint32_t phase = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            const DirHit h = dir_lookup(dir, cap, t);
+            const WenoItem& it = items[h.item];
+            BatchCtl* ctl = it.ctl;
+            s_org[2] = ctl->stepping;
+            if (s_org[2]) {
+                const int tiles_x = (it.g.nx + TX - 1) / TX;
+                const int ty = h.local / tiles_x;
+                s_org[0] = (h.local - ty * tiles_x) * TX;
+                s_org[1] = ty * TY;
+                sa = MixedArgs{it.U[stage - 1], it.U[0], it.U[stage % 3], it.kind, it.gsrc, it.g,
+                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status};
+                s_map = &it.tmap[V][stage - 1];
+                asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
+                                 reinterpret_cast<uint64_t>(s_map))
+                             : "memory");
+            }
+        }
+        __syncthreads();
+        if (s_org[2]) {
+            if (!stage_tile<TY>(s_map, sa, s_org[0], s_org[1], S, &bar, phase)) return;
+            phase ^= 1u;
+        }
+        __syncthreads();
+    }
 }
 
 }  // namespace
+
+cudaError_t launch_weno_stage_mixed_batch(int variant, const WenoItem* items, const int* dir, int cap, int stage,
+                                          int grid, cudaStream_t s) {
+    if (variant == 0)
+        weno_stage_mixed_batch_kernel<0><<<grid, Tile<kWenoTileRows[0]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
+    else
+        weno_stage_mixed_batch_kernel<1><<<grid, Tile<kWenoTileRows[1]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
+    return cudaGetLastError();
+}
+
+int weno_mixed_batch_occupancy(int variant) {
+    int n = 0;
+    if (variant == 0)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_mixed_batch_kernel<0>,
+                                                      Tile<kWenoTileRows[0]>::NTHREAD, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_mixed_batch_kernel<1>,
+                                                      Tile<kWenoTileRows[1]>::NTHREAD, 0);
+    return n;
+}
 
 cudaError_t launch_weno_stage_mixed(const CUtensorMap& tmap, const double* Ucur, const double* Un, double* Uout,
                                     const int8_t* kind, const int32_t* gsrc, const Grid& g, double dtdx,
                                     double dtdy, double gamma, int stage, uint32_t* status, cudaStream_t s) {
     MixedArgs a{Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status};
-    dim3 grid((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY);
-    weno_stage_mixed_kernel<<<grid, NTHREAD, 0, s>>>(tmap, a);
+    dim3 grid((g.nx + TX - 1) / TX, (g.ny + 7) / 8);
+    weno_stage_mixed_kernel<<<grid, Tile<8>::NTHREAD, 0, s>>>(tmap, a);
     return cudaGetLastError();
 }
 
 // Tensor map over one FP64 WENO state: dims (x = nx, y = ny, field = 4),
-// strides pitch*8 and plane*8 bytes, box 40 x 14 x 4.
-bool encode_weno_state_map(CUtensorMap* m, const double* base, const Grid& g, const char** err) {
+// strides pitch*8 and plane*8 bytes, box 40 x (rows + 6) x 4.
+bool encode_weno_state_map(CUtensorMap* m, const double* base, const Grid& g, const char** err, int rows) {
     const uint64_t dims[3] = {(uint64_t)g.nx, (uint64_t)g.ny, 4};
     const uint64_t strides[2] = {(uint64_t)g.pitch * 8, (uint64_t)g.plane * 8};
-    const uint32_t box[3] = {SX, HY, 4};
+    const uint32_t box[3] = {SX, (uint32_t)rows + 6, 4};
     return encode_tmap(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, err);
 }
 
@@ -309,7 +401,7 @@ int zk_weno_mixed_setup(zk_ctx* c) {
     const char* err = nullptr;
     double* bufs[3] = {c->Un, c->S1, c->S2};
     for (int b = 0; b < 3; ++b)
-        if (!zk::encode_weno_state_map(&c->tmap[b], bufs[b], c->g, &err)) return zk_internal_fail(ZK_ERR_CUDA, err);
+        if (!zk::encode_weno_state_map(&c->tmap[b], bufs[b], c->g, &err, 8)) return zk_internal_fail(ZK_ERR_CUDA, err);
     return ZK_OK;
 }
 

@@ -53,6 +53,8 @@ void free_device(zk_ctx* c) {
     c->d_phic = nullptr;
 }
 
+}  // namespace
+
 // Ghost source map on the host, pitched indices.  The reference fills ghosts
 // with a row sweep then a column sweep over the fluid cells
 // (src_WENO/fluid.cpp:338-370, src_DG/fluid.cpp:581-635); a ghost ends up with
@@ -97,6 +99,8 @@ void build_ghost_map(int ny, int nx, int pitch, const int32_t* bct, bool slip, b
             src[k] = s;
         }
 }
+
+namespace {
 
 int check_ctx(zk_ctx* c, bool need_state) {
     if (!c) return fail(ZK_ERR_ARG, "null context");

@@ -44,6 +44,11 @@ struct zk_ctx {
 
 int zk_internal_fail(int code, const char* msg);
 
+// Ghost source map (kind byte and fill source per pitched cell) of a bctype
+// field; slip: DG slip walls (bctype 1); periodic: the -3 ring wraps.
+void build_ghost_map(int ny, int nx, int pitch, const int32_t* bct, bool slip, bool periodic,
+                     std::vector<int8_t>& kind, std::vector<int32_t>& src);
+
 // DG driver (dg_driver.cu)
 int zk_dg_setup(zk_ctx* c);
 void zk_dg_release(zk_ctx* c);
