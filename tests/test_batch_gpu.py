@@ -1,8 +1,9 @@
 """GPU batched runner (zk_batch_*): every problem of a batch -- WENO and DG,
 FP64 and mixed, of different sizes, step counts and CFL numbers, admitted by
 the scheduler at different times -- ends bitwise equal to the same problem run
-alone through zk_step with the time steps the batch chose; the batch's first
-time step follows the reference's CFL rules; a failing problem fails alone."""
+alone through zk_step with the time steps the batch chose; every time step
+follows the reference's CFL rule applied to the max wave speed of the state
+it advances; a failing problem fails alone."""
 import numpy as np
 import pytest
 
@@ -40,17 +41,27 @@ def _specs():
 
 
 def _single(spec, dts):
-    """The same problem alone through zk_step, one step per batch dt."""
+    """The same problem alone through zk_step, one step per batch dt; also
+    the max wave speed (zk_max_speed) of the state before every step."""
     from zuikakucfd_b200 import Solver
     kw = {k: spec[k] for k in ("precision", "limiter", "flux", "boundary") if k in spec}
     with Solver(method=spec["method"], order=spec.get("order", 2), **kw) as s:
         b = spec["bctype"]
         s.set_mesh(b.shape[0], b.shape[1], spec["da"], spec["gamma"], b)
         s.set_state(spec["state"])
-        lam0 = s.max_speed()
+        lams = []
         for dt in dts:
+            lams.append(s.max_speed())
             s.step(float(dt), 1)
-        return s.get_state(), lam0
+        return s.get_state(), lams
+
+
+def _cfl_dt(spec, lam):
+    """The batch's dt rule (WENO cfl da / lambda; DG cfl * dgSafeDt)."""
+    if spec["method"] == "weno":
+        return spec["cfl"] * spec["da"] / lam
+    P = spec["order"]
+    return spec["cfl"] * (0.9 / (2.0 * (2 * P + 1)) * spec["da"] / max(lam, 1e-7))
 
 
 @pytest.mark.parametrize("policy,active,gsteps", [("sjf", 3000.0, 4), ("all", 0.0, 3)])
@@ -68,13 +79,11 @@ def test_batch_matches_single_problems(policy, active, gsteps):
             assert info["status"] & 1 == 0
             dts = bt.dt_history(pid)
             assert np.all(dts > 0) and abs(info["t"] - dts.sum()) <= 1e-12 * dts.sum()
-            ref, lam0 = _single(spec, dts)
-            # first dt from the reference's rules on the initial state
-            if spec["method"] == "weno":
-                assert dts[0] == spec["cfl"] * spec["da"] / lam0
-            else:
-                P = spec["order"]
-                assert dts[0] == spec["cfl"] * (0.9 / (2.0 * (2 * P + 1)) * spec["da"] / max(lam0, 1e-7))
+            ref, lams = _single(spec, dts)
+            # every dt from the reference's max wave speed of the state it
+            # advanced: the first from the reduction launch, the others from
+            # the stage-3 epilogue
+            assert [_cfl_dt(spec, lam) for lam in lams] == list(dts), pid
             got = bt.get_state(pid)
             assert np.array_equal(got, ref), (pid, spec["method"], spec["precision"])
             b = spec["bctype"]
@@ -112,7 +121,10 @@ def test_batch_failure_stays_local():
         assert rep["failed"] == 1 and rep["done"] == 1
         spec = dict(bctype=good.bctype, da=good.da, gamma=good.gamma, state=good.conserved(), method="weno",
                     precision="mixed")
-        ref, _ = _single(spec, bt.dt_history(g))
+        spec["cfl"] = 0.4
+        dts = bt.dt_history(g)
+        ref, lams = _single(spec, dts)
+        assert [_cfl_dt(spec, lam) for lam in lams] == list(dts)
         assert np.array_equal(bt.get_state(g), ref)
 
 

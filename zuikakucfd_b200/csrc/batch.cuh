@@ -36,7 +36,7 @@ struct BatchCtl {
     int stepping;               // 1 while the current step advances this problem
     int method, order;
     uint32_t status;            // STATUS_* bits of this problem's kernels
-    int pad;
+    int lam_ready;              // lam already holds the current state's speed (stage-3 epilogue)
 };
 
 // Tile heights of the WENO stage kernels the autotuner chooses between.
@@ -92,6 +92,61 @@ __device__ __forceinline__ DirHit dir_lookup(const int* __restrict__ dir, int ca
     const int* end = dir + 2 + cap;
     const int s = dir_find(end, n, t);
     return {__ldg(dir + 2 + s), t - (s ? __ldg(end + s - 1) : 0)};
+}
+
+// Wave speed |u| + a of one WENO cell, FP64, with the operations and order of
+// computeMaxSpeed (src_WENO/fluid.cpp:539-553).  The round-to-nearest
+// intrinsics keep it free of FMA contraction in any translation unit, so every
+// kernel that evaluates it gets the bits of the standalone reduction.
+__device__ __forceinline__ double weno_cell_speed(double r, double mx, double my, double E, double gamma) {
+    const double u = __ddiv_rn(mx, r), v = __ddiv_rn(my, r);
+    const double q = __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v));
+    const double p = __dmul_rn(__dsub_rn(gamma, 1.0), __dsub_rn(E, __dmul_rn(__dmul_rn(0.5, r), q)));
+    const double a = __dsqrt_rn(__ddiv_rn(__dmul_rn(gamma, p), r));
+    return __dadd_rn(__dsqrt_rn(q), a);
+}
+
+// Largest corner wave speed of one DG cell (computeMaxSpeedDG_omp,
+// src_DG/solver.cpp:26-64): U at the corners accumulated over the modes in
+// increasing order, floors 1e-12.  cs[k][c] = variable c at corner k.
+__device__ __forceinline__ double dg_cell_speed(const double (&cs)[4][4], double gamma, double umax) {
+    const double eps = 1e-12;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double rho = ref_max(cs[k][0], eps);
+        const double u = __ddiv_rn(cs[k][1], rho), v = __ddiv_rn(cs[k][2], rho);
+        const double q = __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v));
+        const double p =
+            ref_max(__dmul_rn(__dsub_rn(gamma, 1.0), __dsub_rn(cs[k][3], __dmul_rn(__dmul_rn(0.5, rho), q))), eps);
+        const double a = __dsqrt_rn(__ddiv_rn(__dmul_rn(gamma, p), rho));
+        umax = ref_max(umax, __dadd_rn(__dsqrt_rn(q), a));
+    }
+    return umax;
+}
+
+// CTA-wide max of per-thread speeds (>= 0, never NaN) committed with one
+// atomicMax on the bits (the IEEE order of non-negative doubles is the
+// integer order of their bits).  Every thread of the CTA must call it.
+__device__ __forceinline__ void block_max_commit_to(double m, unsigned long long* out) {
+    __shared__ double part[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double x = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (x > m) ? x : m;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = m;
+    __syncthreads();
+    if (warp == 0) {
+        m = (lane < (int)(blockDim.x >> 5)) ? part[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double x = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (x > m) ? x : m;
+        }
+        if (lane == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
 }
 
 __device__ __forceinline__ unsigned long long global_ns() {

@@ -39,6 +39,8 @@ struct DGArgs {
     int hll;             // 1: HLLE instead of HLLC
     double s0;           // Persson threshold -4 log10 P (P<3) or -3 log10 P, from the host's libm
     uint32_t* status;
+    const double* phic;  // basis at the 4 cell corners [NM][4] (want_lam only)
+    int want_lam;        // 1: report the max corner wave speed of the fluid cells written
 };
 
 }  // namespace zk

@@ -386,15 +386,16 @@ __device__ __forceinline__ void limit_cell(double (&o)[4][(P + 1) * (P + 1)], bo
 constexpr int kCellBlock = 64;
 
 // Cells (i, jb + threadIdx.x); sd[v][threadIdx.x] is this thread's (filled)
-// stage input, column-private.
+// stage input, column-private.  Returns the cell's max corner wave speed when
+// want_lam and the cell is fluid (computeMaxSpeedDG_omp), else 0.
 template <int P>
-__device__ __forceinline__ void cell_row(const DGArgs& a, int jb, int i,
-                                         double (&sd)[4 * (P + 1) * (P + 1)][kCellBlock]) {
+__device__ __forceinline__ double cell_row(const DGArgs& a, int jb, int i,
+                                           double (&sd)[4 * (P + 1) * (P + 1)][kCellBlock]) {
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
     const DGTab& T = c_dgtab[P - 1];
     const int t = threadIdx.x;
     const int j = jb + t;
-    if (j >= a.g.nx) return;  // no block-wide synchronisation follows
+    if (j >= a.g.nx) return 0.0;  // no block-wide synchronisation follows
     const int ny = a.g.ny, nx = a.g.nx;
     const size_t plane = a.g.plane, k = (size_t)i * a.g.pitch + j;
     const int8_t kd = a.kind[k] & KIND_MASK;
@@ -469,7 +470,7 @@ __device__ __forceinline__ void cell_row(const DGArgs& a, int jb, int i,
     if (a.stage == 0) {
 #pragma unroll
         for (int v = 0; v < 4 * NM; ++v) a.out[(size_t)v * plane + k] = o[v / NM][v % NM];
-        return;
+        return 0.0;
     }
     // Shu-Osher combine with dt applied (src_DG/fluid.cpp:1024-1026, 1036-1038, 1046-1048)
 #pragma unroll
@@ -495,6 +496,17 @@ __device__ __forceinline__ void cell_row(const DGArgs& a, int jb, int i,
     }
 #pragma unroll
     for (int v = 0; v < 4 * NM; ++v) a.out[(size_t)v * plane + k] = o[v / NM][v % NM];
+    if (!a.want_lam || !(a.kind[k] & KIND_FLUID)) return 0.0;
+    double cs[4][4] = {};
+#pragma unroll
+    for (int m = 0; m < NM; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double b = a.phic[m * 4 + q];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) cs[q][c] += o[c][m] * b;
+        }
+    return dg_cell_speed(cs, a.gamma, 0.0);
 }
 
 template <int P>
@@ -524,6 +536,8 @@ __device__ __forceinline__ DGArgs batch_args(const DgItem& it, int stage) {
     a.hll = it.hll;
     a.s0 = it.s0;
     a.status = &it.ctl->status;
+    a.phic = it.phic;
+    a.want_lam = stage == 3;
     return a;
 }
 
@@ -566,6 +580,7 @@ __global__ void __launch_bounds__(kCellBlock) dg_cell_fp64_batch_kernel(const Dg
     __shared__ double sd[4 * (P + 1) * (P + 1)][kCellBlock];
     __shared__ DGArgs sa;
     __shared__ int s_job[3];  // stepping, row, segment start
+    __shared__ unsigned long long* s_lam;
     const int total = __ldg(dir + 1);
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         if (threadIdx.x == 0) {
@@ -577,10 +592,14 @@ __global__ void __launch_bounds__(kCellBlock) dg_cell_fp64_batch_kernel(const Dg
                 s_job[1] = h.local / segs;
                 s_job[2] = (h.local - s_job[1] * segs) * kCellBlock;
                 sa = batch_args(it, stage);
+                s_lam = &it.ctl->lam;
             }
         }
         __syncthreads();
-        if (s_job[0]) cell_row<P>(sa, s_job[2], s_job[1], sd);
+        if (s_job[0]) {
+            const double m = cell_row<P>(sa, s_job[2], s_job[1], sd);
+            if (stage == 3) block_max_commit_to(m, s_lam);  // the next step's wave speed
+        }
         __syncthreads();
     }
 }

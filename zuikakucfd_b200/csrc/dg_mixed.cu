@@ -51,6 +51,8 @@ struct MixArgs {
     int stage, limiter, hll;
     float s0;
     uint32_t* status;
+    const double* phic;  // basis at the 4 cell corners [NM][4] (LAM kernels only)
+    double gamma64;      // gamma in FP64 (LAM kernels only)
 };
 
 __device__ __forceinline__ float fmaxr(float a, float b) { return (a < b) ? b : a; }
@@ -150,9 +152,11 @@ __device__ __forceinline__ float load_f(const void* p, size_t i) {
 
 // One tile whose top-left cell is (i0, j0), shared memory at `smem`
 // (smem_bytes<P, MTY>()).  Per-thread returns leave only this function: every
-// barrier of the tile precedes them.
-template <int P, typename TIn, typename TOut, int MTY>
-__device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
+// barrier of the tile precedes them.  LAM (FP64 output only): returns the max
+// corner wave speed of the thread's cell if it is fluid (computeMaxSpeedDG_omp
+// on the FP64 values written), else 0.
+template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
+__device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
     constexpr int MNT = MTX * MTY, SY = MTY + 2;
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
     constexpr int SD = SX * SY;  // cell slots of the tile + halo
@@ -286,7 +290,7 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
     // 2. one thread per cell
     const int r = tid / MTX, c = tid - r * MTX;
     const int gi = i0 + r, gj = j0 + c;
-    if (gi >= ny || gj >= nx) return;
+    if (gi >= ny || gj >= nx) return 0.0;
     const int slot = (r + 1) * SX + c + 1;
     const size_t k = (size_t)gi * pitch + gj;
     const uint8_t kd = sk[slot];
@@ -352,7 +356,7 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
     if (a.stage == 0) {
 #pragma unroll
         for (int v = 0; v < 4 * NM; ++v) static_cast<TOut*>(a.out)[(size_t)v * plane + k] = (TOut)acc[v / NM][v % NM];
-        return;
+        return 0.0;
     }
     // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
     const double dt = a.dt;
@@ -449,6 +453,7 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
     }
 
     uint32_t flags = 0;
+    double umax = 0.0;
     if (kd == KIND_UPDATED) {
         if (!isfinite(acc[0][0]) || !isfinite(acc[3][0])) flags |= STATUS_NAN;
         if (!(acc[0][0] > 0.0f)) flags |= STATUS_RHO;
@@ -466,6 +471,7 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
             const double my0 = (1.0 / 3.0) * a.un[(size_t)2 * NM * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + 2 * NM];
             e0 = 1e-5 / (double)(a.gamma - 1.0f) + 0.5 * (mx0 * mx0 + my0 * my0) / rho0;
         }
+        double cs[4][4] = {};  // LAM: variable q at corner e
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -480,7 +486,11 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
                     o *= (double)theta;
                 }
                 out[(size_t)v * plane + k] = (TOut)o;
+                if (LAM)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) cs[e][q] = __dadd_rn(cs[e][q], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
             }
+        if (LAM && (a.kind[k] & KIND_FLUID)) umax = dg_cell_speed(cs, a.gamma64, 0.0);
         if (kd == KIND_UPDATED) {
             const double rho = out[k], mx = out[(size_t)NM * plane + k], my = out[(size_t)2 * NM * plane + k];
             const double p = (double)(a.gamma - 1.0f) * (out[(size_t)3 * NM * plane + k] - 0.5 * (mx * mx + my * my) / rho);
@@ -488,6 +498,7 @@ __device__ __forceinline__ void stage_tile(const MixArgs& a, int j0, int i0, flo
         }
     }
     if (flags) atomicOr(a.status, flags);
+    return umax;
 }
 
 template <int P, int MTY>
@@ -504,7 +515,8 @@ __global__ void __launch_bounds__(MTX * 4, 3) dg_stage_mixed_kernel(MixArgs a) {
 
 // Persistent stage STAGE over every listed problem of a batch group, tile
 // variant V (kDgTileRows[V] rows): stage 1 reads U^n (FP64) and writes F[0],
-// stage 2 reads F[0] and writes F[1], stage 3 reads F[1] and writes U^n.
+// stage 2 reads F[0] and writes F[1], stage 3 reads F[1] and writes U^n and
+// leaves the new state's max wave speed in the problem's control block.
 template <int P, int STAGE, int V>
 __global__ void __launch_bounds__(MTX * kDgTileRows[V], 12 / kDgTileRows[V])
     dg_stage_mixed_batch_kernel(const DgItem* __restrict__ items, const int* __restrict__ dir, int cap) {
@@ -514,6 +526,7 @@ __global__ void __launch_bounds__(MTX * kDgTileRows[V], 12 / kDgTileRows[V])
     extern __shared__ __align__(16) float smem[];
     __shared__ MixArgs sa;  // the current tile's problem, kept out of registers
     __shared__ int s_org[3];
+    __shared__ unsigned long long* s_lam;
     const int total = __ldg(dir + 1);
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         if (threadIdx.x == 0) {
@@ -529,11 +542,15 @@ __global__ void __launch_bounds__(MTX * kDgTileRows[V], 12 / kDgTileRows[V])
                 const void* cur = STAGE == 1 ? (const void*)it.U[0] : (const void*)it.F[STAGE - 2];
                 void* out = STAGE == 3 ? (void*)it.U[0] : (void*)it.F[STAGE - 1];
                 sa = MixArgs{cur, it.U[0], out, it.kind, it.gsrc, it.g, ctl->dt, (float)it.inv2h, (float)it.gamma,
-                             STAGE, it.limiter, it.hll, (float)it.s0, &ctl->status};
+                             STAGE, it.limiter, it.hll, (float)it.s0, &ctl->status, it.phic, it.gamma};
+                s_lam = &ctl->lam;
             }
         }
         __syncthreads();
-        if (s_org[2]) stage_tile<P, TIn, TOut, MTY>(sa, s_org[0], s_org[1], smem);
+        if (s_org[2]) {
+            const double m = stage_tile<P, TIn, TOut, MTY, STAGE == 3>(sa, s_org[0], s_org[1], smem);
+            if (STAGE == 3) block_max_commit_to(m, s_lam);  // the next step's wave speed
+        }
         __syncthreads();
     }
 }

@@ -119,8 +119,9 @@ __global__ void recover_kernel(const double* U, Grid g, size_t vs, double gamma,
 
 constexpr int kRedChunk = 2048;  // cells per reduction tile of the batched runner
 
-// Max wave speed of every listed problem of a batch group that is not finished,
-// committed to its control block (same per-cell semantics as the kernels
+// Max wave speed of every listed problem of a batch group that is not finished
+// and whose speed the previous step's stage 3 did not already leave (first
+// step after admission), committed to its control block (same per-cell semantics as the kernels
 // above; the max is exact, so the tiling does not change the result).
 __global__ void __launch_bounds__(256) max_speed_batch_kernel(const void* __restrict__ items, int method,
                                                               const int* __restrict__ dir, int cap) {
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(256) max_speed_batch_kernel(const void* __rest
         if (method == ZK_METHOD_DG) {
             const DgItem& it = static_cast<const DgItem*>(items)[h.item];
             ctl = it.ctl;
-            if (ctl->state >= BATCH_DONE) continue;
+            if (ctl->state >= BATCH_DONE || ctl->lam_ready) continue;
             const Grid g = it.g;
             const size_t n = (size_t)g.ny * g.nx, c1 = min(n, (size_t)(h.local + 1) * kRedChunk);
             const double eps = 1e-12, gamma = it.gamma;
@@ -155,7 +156,7 @@ __global__ void __launch_bounds__(256) max_speed_batch_kernel(const void* __rest
         } else {
             const WenoItem& it = static_cast<const WenoItem*>(items)[h.item];
             ctl = it.ctl;
-            if (ctl->state >= BATCH_DONE) continue;
+            if (ctl->state >= BATCH_DONE || ctl->lam_ready) continue;
             const Grid g = it.g;
             const double* U = it.U[0];
             const double gamma = it.gamma;
@@ -189,6 +190,7 @@ __global__ void batch_ctl_pre_kernel(BatchCtl* ctl, const int* __restrict__ memb
         c.state = BATCH_RUNNING;
         const double lam = __longlong_as_double((long long)c.lam);
         c.lam = 0ull;
+        c.lam_ready = 0;
         double dt;
         if (c.method == ZK_METHOD_DG) dt = c.cfl * (0.9 / (2.0 * (2 * c.order + 1)) * c.da / ref_max(lam, 1e-7));
         else dt = c.cfl * c.da / lam;
@@ -220,6 +222,8 @@ __global__ void batch_ctl_post_kernel(BatchCtl* ctl, const int* __restrict__ mem
         } else if (c.steps_done >= c.steps_target) {
             c.state = BATCH_DONE;
             c.t_done = global_ns();
+        } else {
+            c.lam_ready = 1;  // stage 3 left the new state's wave speed in lam
         }
     }
 }

@@ -111,6 +111,7 @@ struct StageArgs {
     double dtdx, dtdy, gamma;
     int stage;  // 0: write dU only, 1..3: Shu-Osher stage
     uint32_t* status;
+    int want_lam;  // 1: return the max wave speed of the cells written
 };
 
 template <int TY>
@@ -123,8 +124,9 @@ struct Smem {
 
 // One tile whose top-left cell is (i0, j0).  Ends with every thread past its
 // last shared-memory read, so a persistent caller may reuse S after a barrier.
+// Returns the thread's max wave speed of the cells it wrote (want_lam), else 0.
 template <int TY>
-__device__ __forceinline__ void stage_tile(const StageArgs& a, int j0, int i0, Smem<TY>& S) {
+__device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0, Smem<TY>& S) {
     constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
     auto& sU = S.sU;
     auto& sFx = S.sFx;
@@ -191,6 +193,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int j0, int i0, S
 
     // 3. dU and the stage combine for every cell of the tile
     uint32_t flags = 0;
+    double umax = 0.0;
     for (int t = threadIdx.x; t < TY * TX; t += NTHREAD) {
         const int r = t / TX, c = t - r * TX;
         const int gi = i0 + r, gj = j0 + c;
@@ -225,9 +228,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, int j0, int i0, S
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) a.Uout[q * plane + k] = o[q];
+        if (a.want_lam) {
+            const double spd = weno_cell_speed(o[0], o[1], o[2], o[3], a.gamma);
+            if (spd > umax) umax = spd;
+        }
     }
     flags = __reduce_or_sync(0xffffffffu, flags);
     if (flags && lane == 0) atomicOr(a.status, flags);
+    return umax;
 }
 
 __global__ void __launch_bounds__(Tile<8>::NTHREAD, 2) weno_stage_fp64_kernel(StageArgs a) {
@@ -237,7 +245,8 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 2) weno_stage_fp64_kernel(St
 
 // Persistent stage over every listed problem of a batch group: CTA b takes
 // global tiles b, b + gridDim.x, ...; stage s reads U[s-1] (U^n at stage 1)
-// and writes U[s % 3].
+// and writes U[s % 3].  Stage 3 also leaves the max wave speed of the new
+// state (computeMaxSpeed over all cells) in the problem's control block.
 template <int TY>
 __global__ void __launch_bounds__(Tile<TY>::NTHREAD, 16 / (TY + 1) + 1)
     weno_stage_fp64_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
@@ -245,6 +254,7 @@ __global__ void __launch_bounds__(Tile<TY>::NTHREAD, 16 / (TY + 1) + 1)
     __shared__ Smem<TY> S;
     __shared__ StageArgs sa;  // the current tile's problem, kept out of registers
     __shared__ int s_org[3];  // tile origin x, y; 0 when the problem is not stepping
+    __shared__ unsigned long long* s_lam;
     const int total = __ldg(dir + 1);
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
         if (threadIdx.x == 0) {
@@ -258,11 +268,15 @@ __global__ void __launch_bounds__(Tile<TY>::NTHREAD, 16 / (TY + 1) + 1)
                 s_org[0] = (h.local - ty * tiles_x) * TX;
                 s_org[1] = ty * TY;
                 sa = StageArgs{it.U[stage - 1], it.U[0], it.U[stage % 3], it.kind, it.gsrc, it.g,
-                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status};
+                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status, stage == 3};
+                s_lam = &ctl->lam;
             }
         }
         __syncthreads();
-        if (s_org[2]) stage_tile<TY>(sa, s_org[0], s_org[1], S);
+        if (s_org[2]) {
+            const double m = stage_tile<TY>(sa, s_org[0], s_org[1], S);
+            if (stage == 3) block_max_commit_to(m, s_lam);  // the next step's wave speed
+        }
         __syncthreads();
     }
 }

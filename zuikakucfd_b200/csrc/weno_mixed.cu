@@ -127,6 +127,7 @@ struct MixedArgs {
     double dtdx, dtdy, gamma;
     int stage;
     uint32_t* status;
+    int want_lam;  // 1: report the max wave speed of the cells written
 };
 
 template <int TY>
@@ -141,10 +142,12 @@ struct Smem {
 // One tile whose top-left cell is (i0, j0); `bar` is an initialised mbarrier
 // whose current phase has parity `phase`.  Returns false (after recording
 // STATUS_TIMEOUT) when the TMA copy did not land within the spin limit.
-// Every thread is past its last shared-memory access on return.
+// Every thread is past its last shared-memory access on return.  umax: the
+// thread's max wave speed of the cells it wrote (want_lam), else 0.
 template <int TY>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedArgs& a, int j0, int i0, Smem<TY>& S,
-                                           uint64_t* bar, uint32_t phase) {
+                                           uint64_t* bar, uint32_t phase, double& umax) {
+    umax = 0.0;
     constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
     auto& stg = S.stg;
     auto& sU = S.sU;
@@ -290,6 +293,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) a.Uout[q * plane + k] = o[q];
+        if (a.want_lam) {
+            const double spd = weno_cell_speed(o[0], o[1], o[2], o[3], a.gamma);
+            if (spd > umax) umax = spd;
+        }
     }
     flags = __reduce_or_sync(0xffffffffu, flags);
     if (flags && lane == 0) atomicOr(a.status, flags);
@@ -307,7 +314,8 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 3)
         mbar_init(&bar, 1);
     }
     __syncthreads();
-    stage_tile<8>(&tmap, a, blockIdx.x * TX, blockIdx.y * 8, S, &bar, 0);
+    double umax;
+    stage_tile<8>(&tmap, a, blockIdx.x * TX, blockIdx.y * 8, S, &bar, 0, umax);
 }
 
 // Persistent stage over every listed problem of a batch group (tile variant
@@ -323,6 +331,7 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 24 / (kWenoTi
     __shared__ MixedArgs sa;  // the current tile's problem, kept out of registers
     __shared__ int s_org[3];  // tile origin x, y; 0 when the problem is not stepping
     __shared__ const CUtensorMap* s_map;
+    __shared__ unsigned long long* s_lam;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     const int total = __ldg(dir + 1);
     uint32_t phase = 0;
@@ -338,7 +347,8 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 24 / (kWenoTi
                 s_org[0] = (h.local - ty * tiles_x) * TX;
                 s_org[1] = ty * TY;
                 sa = MixedArgs{it.U[stage - 1], it.U[0], it.U[stage % 3], it.kind, it.gsrc, it.g,
-                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status};
+                               ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status, stage == 3};
+                s_lam = &ctl->lam;
                 s_map = &it.tmap[V][stage - 1];
                 asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
                                  reinterpret_cast<uint64_t>(s_map))
@@ -347,8 +357,10 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 24 / (kWenoTi
         }
         __syncthreads();
         if (s_org[2]) {
-            if (!stage_tile<TY>(s_map, sa, s_org[0], s_org[1], S, &bar, phase)) return;
+            double umax;
+            if (!stage_tile<TY>(s_map, sa, s_org[0], s_org[1], S, &bar, phase, umax)) return;
             phase ^= 1u;
+            if (stage == 3) block_max_commit_to(umax, s_lam);  // the next step's wave speed
         }
         __syncthreads();
     }
