@@ -100,3 +100,20 @@ def test_mixed_smooth_wave_against_exact():
         assert st == 0
         errs[prec] = np.abs(out[0, 0, 3:-3, 3:-3] - ex).mean()
     assert errs["mixed"] <= 1.1 * errs["fp64"], errs
+
+
+def test_l2_projected_wave_convergence_and_mixed_error():
+    """Smooth wave from the L2-projected start (cases.smooth_wave_modes), DG
+    P=2 without limiter to t=0.1 at 32^2 and 64^2: the FP64 density error
+    against the exact cell averages falls at third order, and the mixed path's
+    error stays within 1.1x the FP64 path's at both resolutions."""
+    from zuikakucfd_b200 import accuracy
+    errs = {}
+    for n in (32, 64):
+        r = accuracy.run(n=n, order=2, t_end=0.1, limiter="none")
+        for prec in ("fp64", "mixed"):
+            assert r["paths"][prec]["status_word"] == 0
+        errs[n] = (r["paths"]["fp64"]["rho_l1"], r["paths"]["mixed"]["rho_l1"])
+        assert errs[n][1] <= 1.1 * errs[n][0], (n, errs[n])
+    order = np.log2(errs[32][0] / errs[64][0])
+    assert order > 2.5, (order, errs)

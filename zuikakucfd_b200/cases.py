@@ -165,3 +165,45 @@ def cfl_dt(case: Case, cfl: float = 0.5) -> float:
     a = np.sqrt(case.gamma * case.p / case.rho)
     lam = float(np.max(np.sqrt(case.u ** 2 + case.v ** 2) + a))
     return cfl * case.da / lam
+
+
+def smooth_wave_modes(case: Case, order: int, t: float = 0.0, amplitude: float = 0.2,
+                      length: float = 2.0, nq: int = 6) -> np.ndarray:
+    """L2 projection of the translated smooth wave at time t onto the DG
+    basis, dof[4][NM][ny][nx] (ghost ring included: periodic images).
+
+    The reference initialises mode 0 with the cell-centre value only
+    (src_DG/fluid.cpp:173-182), an O(h^2) start that hides the scheme's order;
+    this projection is the accuracy-study initial condition.  Reference-cell
+    coordinates follow the reference's face convention: xi = +1 is the right
+    face, eta = +1 the face towards row i+1 (downwards, decreasing y).
+    Modes: d_m = (2px+1)(2py+1)/4 * integral of u(xi, eta) P_px(xi) P_py(eta),
+    m = px (P+1) + py, by an nq x nq Gauss rule."""
+    from numpy.polynomial.legendre import leggauss, legval
+    P = int(order)
+    NQ = P + 1
+    nm = NQ * NQ
+    g = case.gamma
+    x, w = leggauss(nq)
+    n = case.nx - 6
+    h = length / n
+    k = np.arange(case.nx)
+    xc = ((k - 3) % n + 0.5) * h
+    yc = length - ((np.arange(case.ny) - 3) % n + 0.5) * h
+    Pv = np.array([legval(x, np.eye(NQ)[p]) for p in range(NQ)])  # [p][q]
+    # density at the nq x nq points of every cell: rho[i, j, a, b]
+    X = xc[None, :, None, None] + 0.5 * h * x[None, None, :, None]
+    Y = yc[:, None, None, None] - 0.5 * h * x[None, None, None, :]
+    rho = 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y - t)))
+    rm = np.zeros((nm,) + rho.shape[:2])
+    for px in range(NQ):
+        for py in range(NQ):
+            wt = (w * Pv[px])[:, None] * (w * Pv[py])[None, :]
+            rm[px * NQ + py] = (2 * px + 1) * (2 * py + 1) / 4.0 * np.einsum("ijab,ab->ij", rho, wt)
+    d = np.zeros((4, nm, case.ny, case.nx))
+    d[0] = rm
+    d[1] = rm            # rho u, u = 1
+    d[2] = rm            # rho v, v = 1
+    d[3] = rm            # E = p/(gamma-1) + rho (u^2+v^2)/2 = 1/(gamma-1) + rho
+    d[3, 0] += 1.0 / (g - 1.0)
+    return d

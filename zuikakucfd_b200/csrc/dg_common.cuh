@@ -18,6 +18,21 @@ struct DGTab {
     double zs[16][DG_MAXNM];                      // Zhang-Shu basis at the 4x4 Gauss points
 };
 
+// One-dimensional factors of P's tensor-product basis phi_m(xi, eta) =
+// P_px(xi) P_py(eta), m = px (P+1) + py, at the NQ = P+1 Gauss points (the
+// 2D quadrature is their tensor grid): L[n][q] = P_n(x_q), D[n][q] = P_n'(x_q),
+// W[q] = w_q, E[n][0|1] = P_n(+1|-1), Z[n][a] = the Zhang-Shu factor of
+// degree n at the 4-point Gauss node a (cubic factor dropped, as the
+// reference's basis() does, src_DG/fluid.cpp:808-823).
+struct DGSep {
+    double L[DG_MAXNQ][DG_MAXNQ];
+    double D[DG_MAXNQ][DG_MAXNQ];
+    double W[DG_MAXNQ];
+    double E[DG_MAXNQ][2];
+    double Z[DG_MAXNQ][4];
+};
+void dg_make_sep(int P, DGSep* S);
+
 // Host: tabulate P's basis (and the 4 corner values used by the CFL
 // reduction, phic[m*4+k]); upload to the calling TU's constant bank.
 void dg_make_tables(int P, DGTab* T, double* phic);

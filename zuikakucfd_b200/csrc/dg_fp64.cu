@@ -110,6 +110,24 @@ void dg_make_tables(int P, DGTab* T, double* phic /* [NM][4] */) {
         for (int k = 0; k < 4; ++k) phic[m * 4 + k] = phi2(m, XI[k], ETA[k]);
 }
 
+void dg_make_sep(int P, DGSep* S) {
+    std::memset(S, 0, sizeof(DGSep));
+    const int NQ = P + 1;
+    for (int n = 0; n < NQ; ++n) {
+        for (int q = 0; q < NQ; ++q) {
+            S->L[n][q] = legP_h(n, kGLPt[NQ][q]);
+            S->D[n][q] = legD_h(n, kGLPt[NQ][q]);
+        }
+        S->E[n][0] = legP_h(n, +1.0);
+        S->E[n][1] = legP_h(n, -1.0);
+        for (int a = 0; a < 4; ++a) {
+            const double x = kGLPt[4][a];
+            S->Z[n][a] = (n == 0) ? 1.0 : (n == 1) ? x : (n == 2) ? 0.5 * (3.0 * x * x - 1.0) : 0.0;
+        }
+    }
+    for (int q = 0; q < NQ; ++q) S->W[q] = kGLWt[NQ][q];
+}
+
 int dg_upload_tables(int P, const DGTab& T) {
     // __constant__ memory is per device: upload once per (device, P)
     static std::mutex mu;

@@ -35,6 +35,17 @@ struct DGTabF {
 
 __constant__ DGTabF c_tabf[3];
 
+// FP32 one-dimensional basis factors (DGSep) for the sum-factorised
+// transforms; WL[n][q] = w_q P_n(x_q).
+struct DGSepF {
+    float L[DG_MAXNQ][DG_MAXNQ];
+    float D[DG_MAXNQ][DG_MAXNQ];
+    float W[DG_MAXNQ];
+    float WL[DG_MAXNQ][DG_MAXNQ];
+    float Z[DG_MAXNQ][4];
+};
+__constant__ DGSepF c_sepf[3];
+
 // A tile is 32 x MTY cells with one thread per cell; shared memory holds the
 // tile plus a 1-cell halo (SX x (MTY + 2) slots).
 constexpr int MTX = 32, SX = MTX + 2;
@@ -161,7 +172,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
     constexpr int SD = SX * SY;  // cell slots of the tile + halo
     constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
-    const DGTabF& T = c_tabf[P - 1];
+    const DGSepF& S = c_sepf[P - 1];
     float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
     float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
     float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
@@ -245,28 +256,57 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
             ydir = true;
         }
         if (sk[sl] != KIND_UPDATED && sk[sr] != KIND_UPDATED) continue;
+        // Traces by sum factorisation: contract the face-normal index with
+        // P_n(+1) = 1 (left/upper cell) and P_n(-1) = (-1)^n (right/lower
+        // cell), then evaluate along the face at the NQ Gauss points.
+        float el[4][NQ], er[4][NQ];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) el[c][n] = er[c][n] = 0.0f;
+        const float* pl = sd + sl * VP;
+        const float* pr = sd + sr * VP;
+        if (ydir) {
+#pragma unroll
+            for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
+                const float4 l4 = *reinterpret_cast<const float4*>(pl + v4);
+                const float4 r4 = *reinterpret_cast<const float4*>(pr + v4);
+                const float lv[4] = {l4.x, l4.y, l4.z, l4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int c = (v4 + e) / NM, m = (v4 + e) % NM, px = m / NQ, py = m % NQ;
+                    el[c][px] += lv[e];
+                    er[c][px] += (py & 1) ? -rv[e] : rv[e];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
+                const float4 l4 = *reinterpret_cast<const float4*>(pl + v4);
+                const float4 r4 = *reinterpret_cast<const float4*>(pr + v4);
+                const float lv[4] = {l4.x, l4.y, l4.z, l4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int c = (v4 + e) / NM, m = (v4 + e) % NM, px = m / NQ, py = m % NQ;
+                    el[c][py] += lv[e];
+                    er[c][py] += (px & 1) ? -rv[e] : rv[e];
+                }
+            }
+        }
         float UL[NQ][4], UR[NQ][4];
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) UL[q][c] = UR[q][c] = 0.0f;
-        const float* pl = sd + sl * VP;
-        const float* pr = sd + sr * VP;
+            for (int c = 0; c < 4; ++c) {
+                float ul = 0.0f, ur = 0.0f;
 #pragma unroll
-        for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
-            const float4 l4 = *reinterpret_cast<const float4*>(pl + v4);
-            const float4 r4 = *reinterpret_cast<const float4*>(pr + v4);
-            const float lv[4] = {l4.x, l4.y, l4.z, l4.w}, rv[4] = {r4.x, r4.y, r4.z, r4.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int c = (v4 + e) / NM, m = (v4 + e) % NM;
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) {
-                    UL[q][c] = fmaf(lv[e], T.tr[side_l][q][m], UL[q][c]);
-                    UR[q][c] = fmaf(rv[e], T.tr[side_r][q][m], UR[q][c]);
+                for (int n = 0; n < NQ; ++n) {
+                    ul = fmaf(el[c][n], S.L[n][q], ul);
+                    ur = fmaf(er[c][n], S.L[n][q], ur);
                 }
+                UL[q][c] = ul;
+                UR[q][c] = ur;
             }
-        }
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
             float Fq[4];
@@ -301,48 +341,102 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         for (int m = 0; m < NM; ++m) acc[q][m] = 0.0f;
     if (kd == KIND_UPDATED) {
         const float* pc = sd + slot * VP;
-#pragma unroll 4
-        for (int p = 0; p < NV; ++p) {
-            float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        // volume integral by sum factorisation over the tensor Gauss grid:
+        // for each xi-row qa, e = d contracted with P_px(x_qa), U at the NQ
+        // points of the row, fluxes, then f = sum_qb w F P_py, g = sum_qb w G P_py',
+        // acc += P_px'(x_qa) f + P_px(x_qa) g
+#pragma unroll
+        for (int qa = 0; qa < NQ; ++qa) {
+            float e[4][NQ];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) e[c][n] = 0.0f;
 #pragma unroll
             for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
                 const float4 d4 = *reinterpret_cast<const float4*>(pc + v4);
                 const float dv[4] = {d4.x, d4.y, d4.z, d4.w};
 #pragma unroll
-                for (int e = 0; e < 4; ++e)
-                    U[(v4 + e) / NM] = fmaf(dv[e], T.vphi[p][(v4 + e) % NM], U[(v4 + e) / NM]);
+                for (int u = 0; u < 4; ++u) {
+                    const int c = (v4 + u) / NM, m = (v4 + u) % NM;
+                    e[c][m % NQ] = fmaf(dv[u], S.L[m / NQ][qa], e[c][m % NQ]);
+                }
             }
-            float F[4], G[4];
-            euler_flux_f(U, a.gamma, F, G);
-            const float w = T.vw[p];
+            float f[4][NQ], g[4][NQ];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) { F[q] *= w; G[q] *= w; }
+            for (int c = 0; c < 4; ++c)
 #pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                const float dxi = T.vdxi[p][m], det = T.vdet[p][m];
+                for (int n = 0; n < NQ; ++n) f[c][n] = g[c][n] = 0.0f;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q][m] = fmaf(F[q], dxi, fmaf(G[q], det, acc[q][m]));
+            for (int qb = 0; qb < NQ; ++qb) {
+                float U[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) x = fmaf(e[c][n], S.L[n][qb], x);
+                    U[c] = x;
+                }
+                float F[4], G[4];
+                euler_flux_f(U, a.gamma, F, G);
+                const float w = S.W[qa] * S.W[qb];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float Fw = F[c] * w, Gw = G[c] * w;
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) {
+                        f[c][n] = fmaf(Fw, S.L[n][qb], f[c][n]);
+                        g[c][n] = fmaf(Gw, S.D[n][qb], g[c][n]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int px = 0; px < NQ; ++px) {
+                const float dx = S.D[px][qa], lx = S.L[px][qa];
+#pragma unroll
+                for (int py = 0; py < NQ; ++py)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        acc[c][px * NQ + py] = fmaf(dx, f[c][py], fmaf(lx, g[c][py], acc[c][px * NQ + py]));
             }
         }
+        // face integrals (src_DG/fluid.cpp:731-796): right (-) and left (+) x
+        // faces weigh the face-normal factor P_px(+1) = 1 and P_px(-1) =
+        // (-1)^px; bottom (-) and top (+) y faces P_py(+-1).  h = sum_q w_q
+        // P_n(x_q) F_q along the face.
+        {
+            const float* Fr = sfx + r * (MTX + 1) + c + 1;
+            const float* Fl = sfx + r * (MTX + 1) + c;
+            const float* Fd = sfy + (r + 1) * MTX + c;
+            const float* Fu = sfy + r * MTX + c;
+            constexpr int fsx = MTY * (MTX + 1), fsy = (MTY + 1) * MTX;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            const float* Fb = (f == 0) ? sfx + r * (MTX + 1) + c + 1
-                            : (f == 1) ? sfx + r * (MTX + 1) + c
-                            : (f == 2) ? sfy + (r + 1) * MTX + c
-                                       : sfy + r * MTX + c;
-            const int fs = (f < 2) ? MTY * (MTX + 1) : (MTY + 1) * MTX;
-            const float sgn = (f == 0 || f == 2) ? -1.0f : 1.0f;
+            for (int u = 0; u < 4; ++u) {
+                float hr[NQ], hl[NQ], hd[NQ], hu[NQ];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                float Fs[4];
+                for (int n = 0; n < NQ; ++n) hr[n] = hl[n] = hd[n] = hu[n] = 0.0f;
 #pragma unroll
-                for (int u = 0; u < 4; ++u) Fs[u] = sgn * Fb[(q * 4 + u) * fs];
+                for (int q = 0; q < NQ; ++q) {
+                    const float xr = Fr[(q * 4 + u) * fsx], xl = Fl[(q * 4 + u) * fsx];
+                    const float xd = Fd[(q * 4 + u) * fsy], xu = Fu[(q * 4 + u) * fsy];
 #pragma unroll
-                for (int m = 0; m < NM; ++m) {
-                    const float bv = T.bv[f][q][m];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) acc[u][m] = fmaf(bv, Fs[u], acc[u][m]);
+                    for (int n = 0; n < NQ; ++n) {
+                        const float wl = S.WL[n][q];
+                        hr[n] = fmaf(wl, xr, hr[n]);
+                        hl[n] = fmaf(wl, xl, hl[n]);
+                        hd[n] = fmaf(wl, xd, hd[n]);
+                        hu[n] = fmaf(wl, xu, hu[n]);
+                    }
                 }
+#pragma unroll
+                for (int px = 0; px < NQ; ++px)
+#pragma unroll
+                    for (int py = 0; py < NQ; ++py) {
+                        float t = acc[u][px * NQ + py] - hr[py] - hd[px];
+                        t += (px & 1) ? -hl[py] : hl[py];
+                        t += (py & 1) ? -hu[px] : hu[px];
+                        acc[u][px * NQ + py] = t;
+                    }
             }
         }
 #pragma unroll
@@ -414,13 +508,27 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         const float rho0 = acc[0][0], mx0 = acc[1][0], my0 = acc[2][0];
         const float ke0 = 0.5f * (mx0 * mx0 + my0 * my0) / rho0;
         if (g1 * (acc[3][0] - ke0) < P_MIN) { acc[3][0] = P_MIN / g1 + ke0; e_fix = true; }
+        // Zhang-Shu points (4 x 4 Gauss grid, cubic factors zero): separable
+        // evaluation, first over px at node a, then over py at node b
+        constexpr int NZ = NQ < 3 ? NQ : 3;
         float th = 1.0f;
 #pragma unroll 1
-        for (int pt = 0; pt < 16; ++pt) {
-            float rho = 0.0f;
+        for (int za = 0; za < 4; ++za) {
+            float t[NZ];
 #pragma unroll
-            for (int m = 0; m < NM; ++m) rho = fmaf(acc[0][m], T.zs[pt][m], rho);
-            if (rho < RHO_MIN) th = fminr(th, (rho0 - RHO_MIN) / (rho0 - rho + EPS));
+            for (int py = 0; py < NZ; ++py) {
+                float x = 0.0f;
+#pragma unroll
+                for (int px = 0; px < NZ; ++px) x = fmaf(acc[0][px * NQ + py], S.Z[px][za], x);
+                t[py] = x;
+            }
+#pragma unroll
+            for (int zb = 0; zb < 4; ++zb) {
+                float rho = 0.0f;
+#pragma unroll
+                for (int py = 0; py < NZ; ++py) rho = fmaf(t[py], S.Z[py][zb], rho);
+                if (rho < RHO_MIN) th = fminr(th, (rho0 - RHO_MIN) / (rho0 - rho + EPS));
+            }
         }
         if (th < 1.0f) {
 #pragma unroll
@@ -431,17 +539,31 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         const float p_avg = g1 * (acc[3][0] - 0.5f * (acc[1][0] * acc[1][0] + acc[2][0] * acc[2][0]) / acc[0][0]);
         float tp = 1.0f;
 #pragma unroll 1
-        for (int pt = 0; pt < 16; ++pt) {
-            float U[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int za = 0; za < 4; ++za) {
+            float t[4][NZ];
 #pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                const float phi = T.zs[pt][m];
+            for (int q = 0; q < 4; ++q)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) U[q] = fmaf(acc[q][m], phi, U[q]);
+                for (int py = 0; py < NZ; ++py) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int px = 0; px < NZ; ++px) x = fmaf(acc[q][px * NQ + py], S.Z[px][za], x);
+                    t[q][py] = x;
+                }
+#pragma unroll
+            for (int zb = 0; zb < 4; ++zb) {
+                float U[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int py = 0; py < NZ; ++py) x = fmaf(t[q][py], S.Z[py][zb], x);
+                    U[q] = x;
+                }
+                if (U[0] <= RHO_MIN) continue;
+                const float p = g1 * (U[3] - 0.5f * (U[1] * U[1] + U[2] * U[2]) / U[0]);
+                if (p < P_MIN) tp = fminr(tp, (p_avg - P_MIN) / (p_avg - p + EPS));
             }
-            if (U[0] <= RHO_MIN) continue;
-            const float p = g1 * (U[3] - 0.5f * (U[1] * U[1] + U[2] * U[2]) / U[0]);
-            if (p < P_MIN) tp = fminr(tp, (p_avg - P_MIN) / (p_avg - p + EPS));
         }
         if (tp < 1.0f) {
 #pragma unroll
@@ -635,6 +757,20 @@ int dg_upload_tables_f32(int P) {
     static_assert(sizeof(DGTab) / sizeof(double) == sizeof(DGTabF) / sizeof(float), "table layouts differ");
     for (size_t i = 0; i < sizeof(DGTab) / sizeof(double); ++i) dst[i] = (float)src[i];
     if (cudaMemcpyToSymbol(c_tabf, &F, sizeof F, sizeof F * (P - 1)) != cudaSuccess) return ZK_ERR_CUDA;
+    DGSep S;
+    dg_make_sep(P, &S);
+    DGSepF SF;
+    std::memset(&SF, 0, sizeof SF);
+    for (int n = 0; n < DG_MAXNQ; ++n) {
+        for (int q = 0; q < DG_MAXNQ; ++q) {
+            SF.L[n][q] = (float)S.L[n][q];
+            SF.D[n][q] = (float)S.D[n][q];
+            SF.WL[n][q] = (float)(S.W[q] * S.L[n][q]);
+        }
+        SF.W[n] = (float)S.W[n];
+        for (int a = 0; a < 4; ++a) SF.Z[n][a] = (float)S.Z[n][a];
+    }
+    if (cudaMemcpyToSymbol(c_sepf, &SF, sizeof SF, sizeof SF * (P - 1)) != cudaSuccess) return ZK_ERR_CUDA;
     done[dev] |= (1ull << P);
     return ZK_OK;
 }
