@@ -40,10 +40,14 @@ def _i(a: np.ndarray):
 
 
 def build(reference: bool = True) -> None:
-    """Compile the restatement and, when the reference sources exist, oracle/_ref."""
+    """Compile the restatement and, when the reference sources exist, oracle/_ref
+    (with the drop-in CLIs once the native library is built)."""
     targets = ["restatement"]
     if reference and Path("/root/reference/src_WENO/fluid.cpp").exists():
         targets.append("ref")
+        lib = HERE.parent / "zuikakucfd_b200" / "lib" / "libzuikaku.so"
+        if lib.exists():  # the reference CLIs linked against the GPU backend
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-C", str(HERE), "-j8", *targets], check=True)
 
 

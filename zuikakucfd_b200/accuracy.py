@@ -5,8 +5,9 @@ exact translated solution and against each other.
     python -m zuikakucfd_b200.accuracy --n 1024 --order 2 --t-end 2 --limiter tvb
 
 rho = 1 + 0.2 sin(pi (x + y)), u = v = p = 1 on [0,2]^2, periodic; the exact
-solution at t is the initial field shifted by (t, t), so at t = 2 it is the
-initial field.  The initial state is the L2 projection onto the DG basis
+solution is rho0(x - t, y + t) (cases.smooth_wave_exact: the solvers' v points
+along increasing row index, downwards), and at t = 2 it is the initial field
+in either orientation.  The initial state is the L2 projection onto the DG basis
 (cases.smooth_wave_modes; --init reference uses the reference's cell-centre
 mode-0 start instead).  dt = 0.9 / (2 (2P+1)) h / lambda, lambda = max |u| + a
 = sqrt(2) + sqrt(gamma p / rho_min), the reference's dgSafeDt at its CFL limit,

@@ -103,7 +103,9 @@ def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0
                 length: float = 2.0) -> Case:
     """rho = 1 + a sin(pi (x + y)), u = v = 1, p = 1 on [0, length]^2, periodic:
     n_interior^2 fluid cells plus a 3-cell ring marked -3 holding the periodic
-    images.  Exact solution at time t: the initial field shifted by (t, t)."""
+    images.  Exact solution at time t: smooth_wave_exact (steady for u = v = 1
+    in the solvers' orientation; periodic in t with period `length` either
+    way)."""
     n = int(n_interior)
     h = length / n
     N = n + 6
@@ -118,12 +120,19 @@ def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0
 
 
 def smooth_wave_exact(case: Case, t: float, amplitude: float = 0.2, length: float = 2.0) -> np.ndarray:
-    """Cell-centre density of the translated wave at time t (interior cells)."""
+    """Cell-centre density of the translated wave at time t (interior cells).
+
+    Both reference solvers difference the y fluxes along increasing row index
+    (the face below minus the face above, src_WENO/fluid.cpp:454-460; the DG
+    bottom face is eta = +1 towards row i+1), so v is the velocity towards
+    increasing row, i.e. downwards in a case file whose row 0 is the top: the
+    exact solution is rho0(x - u t, y + v t).  With u = v = 1 the wave
+    1 + a sin(pi (x + y)) moves along its own crests and is steady."""
     n = case.nx - 6
     h = length / n
     c = (np.arange(n) + 0.5) * h
     X, Y = np.meshgrid(c, length - c)
-    return 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y - t)))
+    return 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y + t)))
 
 
 def high_mach_jet(nx: int = 2048, ny: int = 1024, gamma: float = 5.0 / 3.0, u_jet: float = 30.0,
@@ -194,7 +203,7 @@ def smooth_wave_modes(case: Case, order: int, t: float = 0.0, amplitude: float =
     # density at the nq x nq points of every cell: rho[i, j, a, b]
     X = xc[None, :, None, None] + 0.5 * h * x[None, None, :, None]
     Y = yc[:, None, None, None] - 0.5 * h * x[None, None, None, :]
-    rho = 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y - t)))
+    rho = 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y + t)))  # y + v t: see smooth_wave_exact
     rm = np.zeros((nm,) + rho.shape[:2])
     for px in range(NQ):
         for py in range(NQ):
