@@ -105,8 +105,10 @@ def test_mixed_smooth_wave_against_exact():
 def test_l2_projected_wave_convergence_and_mixed_error():
     """Smooth wave from the L2-projected start (cases.smooth_wave_modes), DG
     P=2 without limiter to t=0.1 at 32^2 and 64^2: the FP64 density error
-    against the exact cell averages falls at third order, and the mixed path's
-    error stays within 1.1x the FP64 path's at both resolutions."""
+    against the exact cell averages falls at third order.  The mixed path's
+    RHS carries FP32 rounding (about 6e-8 of the flux per evaluation), so its
+    error is bounded by max(1.1 x the FP64 error, 2e-7): here, far below the
+    FP32 floor, the floor is what it shows."""
     from zuikakucfd_b200 import accuracy
     errs = {}
     for n in (32, 64):
@@ -114,6 +116,6 @@ def test_l2_projected_wave_convergence_and_mixed_error():
         for prec in ("fp64", "mixed"):
             assert r["paths"][prec]["status_word"] == 0
         errs[n] = (r["paths"]["fp64"]["rho_l1"], r["paths"]["mixed"]["rho_l1"])
-        assert errs[n][1] <= 1.1 * errs[n][0], (n, errs[n])
+        assert errs[n][1] <= max(1.1 * errs[n][0], 2e-7), (n, errs[n])
     order = np.log2(errs[32][0] / errs[64][0])
     assert order > 2.5, (order, errs)

@@ -3,6 +3,7 @@
 exact translated solution and against each other.
 
     python -m zuikakucfd_b200.accuracy --n 1024 --order 2 --t-end 2 --limiter tvb
+    python -m zuikakucfd_b200.accuracy --case jet --steps 2000      # the high-Mach jet
 
 rho = 1 + 0.2 sin(pi (x + y)), u = v = p = 1 on [0,2]^2, periodic; the exact
 solution is rho0(x - t, y + t) (cases.smooth_wave_exact: the solvers' v points
@@ -35,8 +36,10 @@ def exact_cell_average(case: cases.Case, t: float, amplitude: float = 0.2) -> np
 
 
 def run(n: int = 1024, order: int = 2, t_end: float = 2.0, limiter: str = "tvb", init: str = "l2",
-        precisions=("fp64", "mixed"), device: int = 0, chunk: int = 1000) -> dict:
-    w = cases.smooth_wave(n)
+        precisions=("fp64", "mixed"), device: int = 0, chunk: int = 1000, v: float = 1.0) -> dict:
+    """v = 1: the wave as configured (steady in the solvers' orientation);
+    v = -1: translated along the diagonal, back in place at t = 2."""
+    w = cases.smooth_wave(n, v=v)
     P = int(order)
     lam = math.sqrt(2.0) + math.sqrt(w.gamma * 1.0 / 0.8)
     dt0 = 0.9 / (2.0 * (2 * P + 1)) * w.da / lam
@@ -45,7 +48,7 @@ def run(n: int = 1024, order: int = 2, t_end: float = 2.0, limiter: str = "tvb",
     d0 = cases.smooth_wave_modes(w, P) if init == "l2" else w.dg_state(P)
     ex = exact_cell_average(w, t_end)
     out = {"n": n, "order": P, "t_end": t_end, "steps": steps, "dt": dt, "limiter": limiter, "init": init,
-           "paths": {}}
+           "velocity": [1.0, v], "paths": {}}
     states = {}
     for prec in precisions:
         with Solver(method="dg", order=P, precision=prec, limiter=limiter, boundary="periodic",
@@ -78,6 +81,51 @@ def run(n: int = 1024, order: int = 2, t_end: float = 2.0, limiter: str = "tvb",
     return out
 
 
+def jet(nx: int = 2048, ny: int = 1024, steps: int = 2000, weno_cfl=(0.003, 0.01, 0.03), dg_cfl=(1.0,),
+        precisions=("fp64", "mixed"), device: int = 0) -> dict:
+    """The high-Mach jet (cases.high_mach_jet: rho = 5, u = 30 band, gamma =
+    5/3, about Mach 80) advanced `steps` steps with WENO5 at each CFL number in
+    weno_cfl (dt = cfl da / lambda0, the reference driver's fixed-dt form) and
+    with DG P=1 at each dg_cfl x dgSafeDt (Persson + Zhang-Shu limiter), FP64 and
+    mixed precision.  Per run: the device status word (1 NaN, 2 rho <= 0,
+    4 p <= 0 seen), min density and pressure of the final cell averages, time;
+    per method and CFL: mixed-vs-FP64 L1 / L-inf differences of rho and p."""
+    c = cases.high_mach_jet(nx, ny)
+    a_jet = math.sqrt(c.gamma * 0.4127 / 5.0)
+    lam0 = 30.0 + a_jet
+    runs = []
+    for method, order, cfls in (("weno", 2, weno_cfl), ("dg", 1, tuple(dg_cfl))):
+        for cfl in cfls:
+            dt = cfl * c.da / lam0 if method == "weno" else cfl * 0.9 / (2.0 * 3.0) * c.da / lam0
+            res, prim = {}, {}
+            for prec in precisions:
+                with Solver(method=method, order=order, precision=prec, device=device) as s:
+                    s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
+                    s.set_state(c.conserved() if method == "weno" else c.dg_state(order))
+                    t0 = time.perf_counter()
+                    s.step(dt, steps)
+                    s.synchronize()
+                    secs = time.perf_counter() - t0
+                    q = s.recover_primitives()
+                    st = s.status_word()
+                rho, p = q[0][3:-3, 3:-3], q[3][3:-3, 3:-3]
+                fin = bool(np.isfinite(rho).all() and np.isfinite(p).all())
+                prim[prec] = (rho, p)
+                res[prec] = {"status_word": st, "finite": fin, "seconds": secs,
+                             "rho_min": float(np.nanmin(rho)), "p_min": float(np.nanmin(p))}
+            row = {"method": method, "order": order if method == "dg" else None, "cfl": cfl, "dt": dt,
+                   "steps": steps, "paths": res}
+            if len(prim) == 2 and all(v["finite"] for v in res.values()):
+                (r64, p64), (rmx, pmx) = prim["fp64"], prim["mixed"]
+                row["mixed_vs_fp64"] = {
+                    "rho_l1_rel": float(np.abs(rmx - r64).sum() / np.abs(r64).sum()),
+                    "rho_linf": float(np.abs(rmx - r64).max()),
+                    "p_l1_rel": float(np.abs(pmx - p64).sum() / np.abs(p64).sum()),
+                    "p_linf": float(np.abs(pmx - p64).max())}
+            runs.append(row)
+    return {"case": f"high-Mach jet {nx}x{ny}", "runs": runs}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--n", type=int, default=1024)
@@ -86,8 +134,16 @@ def main(argv=None) -> int:
     ap.add_argument("--limiter", default="tvb")
     ap.add_argument("--init", default="l2", choices=["l2", "reference"])
     ap.add_argument("--precisions", default="fp64,mixed")
+    ap.add_argument("--case", default="wave", choices=["wave", "jet"])
+    ap.add_argument("--steps", type=int, default=2000, help="jet: steps per run")
+    ap.add_argument("--v", type=float, default=1.0, help="wave: row-direction velocity (-1: translating)")
+    ap.add_argument("--dg-cfl", default="1.0", help="jet: comma-separated multiples of dgSafeDt for DG P=1")
     a = ap.parse_args(argv)
-    print(json.dumps(run(a.n, a.order, a.t_end, a.limiter, a.init, a.precisions.split(","))), flush=True)
+    if a.case == "jet":
+        print(json.dumps(jet(steps=a.steps, precisions=a.precisions.split(","),
+                             dg_cfl=tuple(float(x) for x in a.dg_cfl.split(",")))), flush=True)
+        return 0
+    print(json.dumps(run(a.n, a.order, a.t_end, a.limiter, a.init, a.precisions.split(","), v=a.v)), flush=True)
     return 0
 
 

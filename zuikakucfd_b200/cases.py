@@ -100,7 +100,7 @@ def four_quadrant(n: int = 256, seed: int = 0, gamma: float = 1.4, ny: int | Non
 
 
 def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0.2,
-                length: float = 2.0) -> Case:
+                length: float = 2.0, u: float = 1.0, v: float = 1.0) -> Case:
     """rho = 1 + a sin(pi (x + y)), u = v = 1, p = 1 on [0, length]^2, periodic:
     n_interior^2 fluid cells plus a 3-cell ring marked -3 holding the periodic
     images.  Exact solution at time t: smooth_wave_exact (steady for u = v = 1
@@ -115,7 +115,7 @@ def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0
     X, Y = np.meshgrid(xc, yc)
     rho = 1.0 + amplitude * np.sin(np.pi * (X + Y))
     one = np.ones((N, N))
-    return Case(f"smooth_wave_{n}", N, N, h, gamma, rho, one.copy(), one.copy(), one.copy(),
+    return Case(f"smooth_wave_{n}", N, N, h, gamma, rho, u * one, v * one, one.copy(),
                 _ring(N, N, 3, -3), periodic=True)
 
 
@@ -127,12 +127,14 @@ def smooth_wave_exact(case: Case, t: float, amplitude: float = 0.2, length: floa
     bottom face is eta = +1 towards row i+1), so v is the velocity towards
     increasing row, i.e. downwards in a case file whose row 0 is the top: the
     exact solution is rho0(x - u t, y + v t).  With u = v = 1 the wave
-    1 + a sin(pi (x + y)) moves along its own crests and is steady."""
+    1 + a sin(pi (x + y)) moves along its own crests and is steady; v = -1
+    translates it along the diagonal."""
     n = case.nx - 6
     h = length / n
     c = (np.arange(n) + 0.5) * h
     X, Y = np.meshgrid(c, length - c)
-    return 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y + t)))
+    u, v = float(case.u.flat[0]), float(case.v.flat[0])
+    return 1.0 + amplitude * np.sin(np.pi * ((X - u * t) + (Y + v * t)))
 
 
 def high_mach_jet(nx: int = 2048, ny: int = 1024, gamma: float = 5.0 / 3.0, u_jet: float = 30.0,
@@ -203,7 +205,8 @@ def smooth_wave_modes(case: Case, order: int, t: float = 0.0, amplitude: float =
     # density at the nq x nq points of every cell: rho[i, j, a, b]
     X = xc[None, :, None, None] + 0.5 * h * x[None, None, :, None]
     Y = yc[:, None, None, None] - 0.5 * h * x[None, None, None, :]
-    rho = 1.0 + amplitude * np.sin(np.pi * ((X - t) + (Y + t)))  # y + v t: see smooth_wave_exact
+    u, v = float(case.u.flat[0]), float(case.v.flat[0])
+    rho = 1.0 + amplitude * np.sin(np.pi * ((X - u * t) + (Y + v * t)))  # y + v t: see smooth_wave_exact
     rm = np.zeros((nm,) + rho.shape[:2])
     for px in range(NQ):
         for py in range(NQ):
@@ -211,8 +214,8 @@ def smooth_wave_modes(case: Case, order: int, t: float = 0.0, amplitude: float =
             rm[px * NQ + py] = (2 * px + 1) * (2 * py + 1) / 4.0 * np.einsum("ijab,ab->ij", rho, wt)
     d = np.zeros((4, nm, case.ny, case.nx))
     d[0] = rm
-    d[1] = rm            # rho u, u = 1
-    d[2] = rm            # rho v, v = 1
-    d[3] = rm            # E = p/(gamma-1) + rho (u^2+v^2)/2 = 1/(gamma-1) + rho
-    d[3, 0] += 1.0 / (g - 1.0)
+    d[1] = u * rm                      # rho u (u, v, p constant)
+    d[2] = v * rm                      # rho v
+    d[3] = 0.5 * (u * u + v * v) * rm  # E = p/(gamma-1) + rho (u^2+v^2)/2
+    d[3, 0] += float(case.p.flat[0]) / (g - 1.0)
     return d

@@ -182,6 +182,18 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
 
+    // U^n of this thread's cell is read again only by the combine: start
+    // bringing it into L2 now so those loads overlap the flux work
+    {
+        const int pr = tid / MTX, pc = tid - pr * MTX;
+        if (i0 + pr < ny && j0 + pc < nx) {
+            const double* u0 = a.un + (size_t)(i0 + pr) * pitch + (j0 + pc);
+#pragma unroll 8
+            for (int v = 0; v < 4 * NM; ++v)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(u0 + (size_t)v * plane));
+        }
+    }
+
     // 0. gather tile + halo (corners unused)
     for (int slot = tid; slot < SD; slot += MNT) {
         const int r = slot / SX, c = slot - r * SX;
