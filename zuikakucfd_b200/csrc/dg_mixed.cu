@@ -169,7 +169,7 @@ __device__ __forceinline__ float load_f(const void* p, size_t i) {
 template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
 __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
     constexpr int MNT = MTX * MTY, SY = MTY + 2;
-    constexpr int NQ = P + 1, NM = NQ * NQ, NV = NQ * NQ;
+    constexpr int NQ = P + 1, NM = NQ * NQ;
     constexpr int SD = SX * SY;  // cell slots of the tile + halo
     constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
     const DGSepF& S = c_sepf[P - 1];
@@ -357,7 +357,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         // for each xi-row qa, e = d contracted with P_px(x_qa), U at the NQ
         // points of the row, fluxes, then f = sum_qb w F P_py, g = sum_qb w G P_py',
         // acc += P_px'(x_qa) f + P_px(x_qa) g
-#pragma unroll
+#pragma unroll 1
         for (int qa = 0; qa < NQ; ++qa) {
             float e[4][NQ];
 #pragma unroll
