@@ -139,6 +139,58 @@ struct Smem {
     uint8_t sK[TY + 6][HX];     // kind | HIGH_MACH
 };
 
+// Flux of one face: XDIR, the x face left of tile cell (r, c) (stencil cells
+// (r, c-3 .. c+2)); else the y face above it (cells (r-3 .. r+2, c), normal
+// momentum swapped into slot 1).  FP32 unless a stencil cell is high-Mach.
+template <bool XDIR, int TY>
+__device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamma, float gf) {
+    constexpr int SU = XDIR ? 1 : HX;  // stride between stencil cells in sU / sK
+    constexpr int SG = XDIR ? 1 : SX;  // and in stg
+    const float* u0 = XDIR ? &S.sU[0][r + 3][c] : &S.sU[0][r][c + 3];
+    const uint8_t* k0 = XDIR ? &S.sK[r + 3][c] : &S.sK[r][c + 3];
+    constexpr int PU = (TY + 6) * HX;  // plane stride of sU
+    uint8_t hm = 0;
+#pragma unroll
+    for (int n = 0; n < 6; ++n) hm |= k0[n * SU];
+    double F[4];
+    if (hm & HIGH_MACH) {
+        const double* g0 = XDIR ? &S.stg[0][r + 3][c + 1] : &S.stg[0][r][c + 4];
+        constexpr int PG = (TY + 6) * SX;
+        double QL[4], QR[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const double* g = g0 + q * PG;
+            weno5<double>(g[0], g[SG], g[2 * SG], g[3 * SG], g[4 * SG], g[5 * SG], QL[q], QR[q]);
+        }
+        if (!XDIR) {
+            double t = QL[1]; QL[1] = QL[2]; QL[2] = t;
+            t = QR[1]; QR[1] = QR[2]; QR[2] = t;
+        }
+        hllc<double>(QL, QR, gamma, F);
+    } else {
+        float QL[4], QR[4], Ff[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float* u = u0 + q * PU;
+            weno5<float>(u[0], u[SU], u[2 * SU], u[3 * SU], u[4 * SU], u[5 * SU], QL[q], QR[q]);
+        }
+        if (!XDIR) {
+            float t = QL[1]; QL[1] = QL[2]; QL[2] = t;
+            t = QR[1]; QR[1] = QR[2]; QR[2] = t;
+        }
+        hllc<float>(QL, QR, gf, Ff);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) F[q] = (double)Ff[q];
+    }
+    if (XDIR) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) S.sFx[q][r][c] = F[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) S.sFy[q][r][c] = F[q];
+    }
+}
+
 // One tile whose top-left cell is (i0, j0); `bar` is an initialised mbarrier
 // whose current phase has parity `phase`.  Returns false (after recording
 // STATUS_TIMEOUT) when the TMA copy did not land within the spin limit.
@@ -206,57 +258,20 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const float gf = (float)a.gamma;
     for (int task = warp; task < 2 * TY + 2; task += NWARP) {
-        const bool xdir = task <= TY;
-        int r, c;
-        if (xdir) {
+        // a task is one row of x faces or of y faces, so the direction is
+        // uniform across the warp and the stencil addressing is compile-time
+        if (task <= TY) {
+            int r, c;
             if (task < TY) { r = task; c = lane; }
             else { if (lane >= TY) continue; r = lane; c = TX; }
             if ((sK[r + 3][c + 2] & KIND_MASK) != KIND_UPDATED && (sK[r + 3][c + 3] & KIND_MASK) != KIND_UPDATED)
                 continue;
+            face_flux<true, TY>(S, r, c, a.gamma, gf);
         } else {
-            r = task - TY - 1; c = lane;
+            const int r = task - TY - 1, c = lane;
             if ((sK[r + 2][c + 3] & KIND_MASK) != KIND_UPDATED && (sK[r + 3][c + 3] & KIND_MASK) != KIND_UPDATED)
                 continue;
-        }
-        // stencil cell n (0..5) at smem (rr, cc)
-        auto R_ = [&](int n) { return xdir ? r + 3 : r + n; };
-        auto C_ = [&](int n) { return xdir ? c + n : c + 3; };
-        uint8_t hm = 0;
-#pragma unroll
-        for (int n = 0; n < 6; ++n) hm |= sK[R_(n)][C_(n)];
-        double F[4];
-        if (hm & HIGH_MACH) {
-            double QL[4], QR[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                weno5<double>(stg[q][R_(0)][C_(0) + 1], stg[q][R_(1)][C_(1) + 1], stg[q][R_(2)][C_(2) + 1],
-                              stg[q][R_(3)][C_(3) + 1], stg[q][R_(4)][C_(4) + 1], stg[q][R_(5)][C_(5) + 1],
-                              QL[q], QR[q]);
-            if (!xdir) {
-                double t = QL[1]; QL[1] = QL[2]; QL[2] = t;
-                t = QR[1]; QR[1] = QR[2]; QR[2] = t;
-            }
-            hllc<double>(QL, QR, a.gamma, F);
-        } else {
-            float QL[4], QR[4], Ff[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                weno5<float>(sU[q][R_(0)][C_(0)], sU[q][R_(1)][C_(1)], sU[q][R_(2)][C_(2)], sU[q][R_(3)][C_(3)],
-                             sU[q][R_(4)][C_(4)], sU[q][R_(5)][C_(5)], QL[q], QR[q]);
-            if (!xdir) {
-                float t = QL[1]; QL[1] = QL[2]; QL[2] = t;
-                t = QR[1]; QR[1] = QR[2]; QR[2] = t;
-            }
-            hllc<float>(QL, QR, gf, Ff);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) F[q] = (double)Ff[q];
-        }
-        if (xdir) {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sFx[q][r][c] = F[q];
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) sFy[q][r][c] = F[q];
+            face_flux<false, TY>(S, r, c, a.gamma, gf);
         }
     }
     __syncthreads();
