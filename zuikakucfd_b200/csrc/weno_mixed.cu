@@ -224,6 +224,16 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
         return false;
     }
 
+    // U^n of the tile is read again only by the combine; at stages 2 and 3 it
+    // is not the TMA'd buffer, so start it towards L2 now (each 32-cell row
+    // segment of a plane is two 128-byte lines; pitch is a multiple of 32)
+    if (a.stage >= 2 && threadIdx.x < 8 * TY) {
+        const int q = threadIdx.x / (2 * TY), rr = (threadIdx.x >> 1) - q * TY, half = threadIdx.x & 1;
+        if (i0 + rr < ny)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(a.Un + q * plane + (size_t)(i0 + rr) * pitch + j0 +
+                                                          16 * half));
+    }
+
     // 2. ghost fill from the source map, FP32 copy, high-Mach flags
     const double gm1 = a.gamma - 1.0;
     for (int t = threadIdx.x; t < HY * HX; t += NTHREAD) {
@@ -244,9 +254,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
                     stg[q][r][c + 1] = v[q];
                 }
             }
-            const double ke = 0.5 * (v[1] * v[1] + v[2] * v[2]) / v[0];
-            const double p = gm1 * (v[3] - ke);
-            if (!(p > 0.0) || v[3] > 100.0 * p) kd |= HIGH_MACH;
+            // high-Mach test E > 100 p, p = (gamma-1)(E - |m|^2 / 2 rho), with
+            // both sides multiplied by rho > 0 (no division)
+            const double prho = gm1 * (v[3] * v[0] - 0.5 * (v[1] * v[1] + v[2] * v[2]));
+            if (!(v[0] > 0.0) || !(prho > 0.0) || v[3] * v[0] > 100.0 * prho) kd |= HIGH_MACH;
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) sU[q][r][c] = (float)v[q];
