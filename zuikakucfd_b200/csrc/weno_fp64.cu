@@ -238,7 +238,8 @@ __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0,
     return umax;
 }
 
-__global__ void __launch_bounds__(Tile<8>::NTHREAD, 2) weno_stage_fp64_kernel(StageArgs a) {
+// 3 CTAs per SM (72 registers, no spills): +19% over 2 CTAs at 84 registers.
+__global__ void __launch_bounds__(Tile<8>::NTHREAD, 3) weno_stage_fp64_kernel(StageArgs a) {
     __shared__ Smem<8> S;
     stage_tile<8>(a, blockIdx.x * TX, blockIdx.y * 8, S);
 }
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 2) weno_stage_fp64_kernel(St
 // and writes U[s % 3].  Stage 3 also leaves the max wave speed of the new
 // state (computeMaxSpeed over all cells) in the problem's control block.
 template <int TY>
-__global__ void __launch_bounds__(Tile<TY>::NTHREAD, 16 / (TY + 1) + 1)
+__global__ void __launch_bounds__(Tile<TY>::NTHREAD, 864 / Tile<TY>::NTHREAD)
     weno_stage_fp64_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
                                  int stage) {
     __shared__ Smem<TY> S;
