@@ -331,9 +331,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
     return true;
 }
 
-// 4 CTAs per SM (56 registers, a few spilled): the extra resident warps hide
-// more latency than the spills cost (+14% over 3 CTAs at 72 registers).
-__global__ void __launch_bounds__(Tile<8>::NTHREAD, 4)
+// 5 CTAs per SM (40 registers, some spilled; 223 KB of shared memory): the
+// extra resident warps hide more latency than the spills cost (+14% at 4 CTAs
+// and +2.4% more at 5, over 3 CTAs at 72 registers).
+__global__ void __launch_bounds__(Tile<8>::NTHREAD, 5)
     weno_stage_mixed_kernel(const __grid_constant__ CUtensorMap tmap, MixedArgs a) {
     __shared__ __align__(128) Smem<8> S;
     __shared__ __align__(8) uint64_t bar;
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 4)
 // v: kWenoTileRows[v] rows).  The tensor maps live in the item array in
 // global memory, written by the host before the launch.
 template <int V>
-__global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1152 / Tile<kWenoTileRows[V]>::NTHREAD)
+__global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1440 / Tile<kWenoTileRows[V]>::NTHREAD)
     weno_stage_mixed_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
                                   int stage) {
     constexpr int TY = kWenoTileRows[V];
