@@ -641,8 +641,10 @@ constexpr size_t smem_bytes() {
     return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
 }
 
+// resident CTAs per SM: 8 for P=1 (+5% over 3), 3 for P=2 (4 and 5 were
+// slower) and P=3 (bounded by shared memory)
 template <int P, typename TIn, typename TOut>
-__global__ void __launch_bounds__(MTX * 4, 3) dg_stage_mixed_kernel(MixArgs a) {
+__global__ void __launch_bounds__(MTX * 4, P == 1 ? 8 : 3) dg_stage_mixed_kernel(MixArgs a) {
     extern __shared__ __align__(16) float smem[];
     stage_tile<P, TIn, TOut, 4>(a, blockIdx.x * MTX, blockIdx.y * 4, smem);
 }
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(MTX * 4, 3) dg_stage_mixed_kernel(MixArgs a) {
 // stage 2 reads F[0] and writes F[1], stage 3 reads F[1] and writes U^n and
 // leaves the new state's max wave speed in the problem's control block.
 template <int P, int STAGE, int V>
-__global__ void __launch_bounds__(MTX * kDgTileRows[V], 12 / kDgTileRows[V])
+__global__ void __launch_bounds__(MTX * kDgTileRows[V], (P == 1 ? 32 : 12) / kDgTileRows[V])
     dg_stage_mixed_batch_kernel(const DgItem* __restrict__ items, const int* __restrict__ dir, int cap) {
     constexpr int MTY = kDgTileRows[V];
     using TIn = typename std::conditional<STAGE == 1, double, float>::type;
