@@ -114,6 +114,11 @@ int zk_max_speed(zk_ctx* ctx, double* out);
  * rho, u, v, p of the cell averages, FP64. */
 int zk_recover_primitives(zk_ctx* ctx, double* host_prim);
 
+/* Mach number mach[ny][nx] = |u| / sqrt(gamma p / rho) and speed[ny][nx] =
+ * |u| (may be NULL) of the cell averages, computed on the device (the plot
+ * notebook's compute_mach, plot.ipynb cell 0; no counterpart in the solver). */
+int zk_mach_number(zk_ctx* ctx, double* host_mach, double* host_speed);
+
 /* Device status word (bit 0: NaN seen, bit 1: rho <= 0, bit 2: p <= 0) of the
  * last zk_step; cleared by each zk_step. */
 int zk_status_word(zk_ctx* ctx, uint32_t* out);

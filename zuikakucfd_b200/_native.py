@@ -100,6 +100,7 @@ _SIGS = {
     "zk_weno_step_noalloc": (C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.POINTER(C.c_int32), C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_uint32)]),
+    "zk_mach_number": (C.c_int, [_P, _D, _D]),
     "zk_batch_default_options": (None, [C.POINTER(zk_batch_options)]),
     "zk_batch_create": (C.c_int, [C.POINTER(zk_batch_options), C.POINTER(_P)]),
     "zk_batch_add": (C.c_int, [_P, C.POINTER(zk_options), C.c_int, C.c_int, C.c_double, C.c_double,

@@ -99,6 +99,47 @@ def four_quadrant(n: int = 256, seed: int = 0, gamma: float = 1.4, ny: int | Non
                 f[..., 2], f[..., 3], _ring(gy, gx, 3, ring_code), seed=seed)
 
 
+def riemann_config(n: int = 512, gamma: float = 1.4, ny: int | None = None, split: float = 0.85) -> Case:
+    """The generator notebook's fixed four-quadrant Riemann configuration
+    (gen.ipynb cell 0): interfaces at x = y = split on [0,1]^2 (row 0 on top),
+    NE (1.5, 0, 0, 1.5), NW (0.5323, 1.206, 0, 0.3), SW (0.138, 1.206, -1.206,
+    0.029), SE (0.5323, 0, -1.206, 0.3) as (rho, u, v, p); 3-cell -1 ring.
+    The reference's shipped 2D-Riemann case is this configuration at n = 256
+    with split = 0.8 (its interfaces lie between columns 204/205 and rows
+    50/51); the notebook's default is 0.85."""
+    nx = int(n)
+    ny = int(ny or n)
+    da = 1.0 / nx
+    xc = (np.arange(nx) + 0.5) * da
+    yc = 1.0 - (np.arange(ny) + 0.5) * da
+    X, Y = np.meshgrid(xc, yc)
+    east, north = X >= split, Y >= split
+    tab = np.array([(1.5, 0.0, 0.0, 1.5), (0.5323, 1.206, 0.0, 0.3), (0.138, 1.206, -1.206, 0.029),
+                    (0.5323, 0.0, -1.206, 0.3)])
+    f = tab[np.where(north & east, 0, np.where(north, 1, np.where(east, 3, 2)))]
+    return Case(f"riemann_config_{nx}x{ny}", ny, nx, da, gamma, f[..., 0], f[..., 1], f[..., 2], f[..., 3],
+                _ring(ny, nx, 3, -1))
+
+
+def center_detonation(n: int = 1024, gamma: float = 1.4, domain: float = 2000.0, R0: float = 10.0,
+                      rho_in: float = 0.1, p_in: float = 1e10, rho_out: float = 1.225,
+                      p_out: float = 101325.0) -> Case:
+    """The generator notebook's centre detonation (gen.ipynb cell 1), SI units:
+    a disc of radius R0 at the centre of [0, domain]^2 holding (rho_in, p_in)
+    in air at rest (rho_out, p_out); 2-cell -1 ring, as the notebook writes."""
+    nx = ny = int(n)
+    da = domain / nx
+    xc = (np.arange(nx) + 0.5) * da
+    yc = domain - (np.arange(ny) + 0.5) * da
+    X, Y = np.meshgrid(xc, yc)
+    inside = (X - domain / 2.0) ** 2 + (Y - domain / 2.0) ** 2 <= R0 * R0
+    rho = np.where(inside, rho_in, rho_out)
+    p = np.where(inside, p_in, p_out)
+    zero = np.zeros((ny, nx))
+    return Case(f"center_detonation_{nx}", ny, nx, da, gamma, rho, zero.copy(), zero.copy(), p,
+                _ring(ny, nx, 2, -1))
+
+
 def smooth_wave(n_interior: int = 1024, gamma: float = 1.4, amplitude: float = 0.2,
                 length: float = 2.0, u: float = 1.0, v: float = 1.0) -> Case:
     """rho = 1 + a sin(pi (x + y)), u = v = 1, p = 1 on [0, length]^2, periodic:
@@ -219,3 +260,32 @@ def smooth_wave_modes(case: Case, order: int, t: float = 0.0, amplitude: float =
     d[3] = 0.5 * (u * u + v * v) * rm  # E = p/(gamma-1) + rho (u^2+v^2)/2
     d[3, 0] += float(case.p.flat[0]) / (g - 1.0)
     return d
+
+
+GENERATORS = {
+    "four_quadrant": lambda a: four_quadrant(a.n, seed=a.seed),
+    "riemann_config": lambda a: riemann_config(a.n),
+    "center_detonation": lambda a: center_detonation(a.n),
+    "smooth_wave": lambda a: smooth_wave(a.n),
+    "high_mach_jet": lambda a: high_mach_jet(a.n, a.n // 2),
+}
+
+
+def main(argv=None) -> int:
+    """Write a case folder in the reference's format:
+    python -m zuikakucfd_b200.cases <generator> --n N [--seed S] --out DIR"""
+    import argparse
+    ap = argparse.ArgumentParser(description=main.__doc__.splitlines()[0])
+    ap.add_argument("generator", choices=sorted(GENERATORS))
+    ap.add_argument("--n", type=int, default=256, help="cells per side (interior cells for smooth_wave)")
+    ap.add_argument("--seed", type=int, default=0, help="four_quadrant: RNG seed")
+    ap.add_argument("--out", required=True)
+    a = ap.parse_args(argv)
+    c = GENERATORS[a.generator](a)
+    d = write_case(c, a.out)
+    print(f"{c.name}: {c.ny}x{c.nx}, da={c.da:.6g}, gamma={c.gamma} -> {d}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

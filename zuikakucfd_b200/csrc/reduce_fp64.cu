@@ -115,6 +115,23 @@ __global__ void recover_kernel(const double* U, Grid g, size_t vs, double gamma,
     }
 }
 
+// Mach number and speed of the cell averages, the plot notebook's
+// compute_mach (plot.ipynb cell 0): |u| / sqrt(gamma p / rho), p recovered as
+// recoverPrimitives does.  U points at variable 0 (mode 0 for DG); vs = plane
+// stride between variables.
+__global__ void mach_kernel(const double* U, Grid g, size_t vs, double gamma, double* mach, double* speed) {
+    const size_t n = (size_t)g.ny * g.nx;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t i = t / g.nx, j = t - i * g.nx, k = i * g.pitch + j;
+        const double rho = U[k], ux = U[vs + k] / rho, vy = U[2 * vs + k] / rho;
+        const double p = (gamma - 1.0) * (U[3 * vs + k] - 0.5 * rho * (ux * ux + vy * vy));
+        const double vel = sqrt(ux * ux + vy * vy);
+        speed[k] = vel;
+        mach[k] = vel / sqrt(gamma * p / rho);
+    }
+}
+
 // ---- batched runner: per-problem CFL reductions and step control ---------------
 
 constexpr int kRedChunk = 2048;  // cells per reduction tile of the batched runner
@@ -266,6 +283,12 @@ cudaError_t launch_max_speed_dg(const double* dof, const int8_t* kind, const Gri
 cudaError_t launch_recover(const double* U, const Grid& g, int nm, double gamma, double* prim,
                            int sms, cudaStream_t s) {
     recover_kernel<<<grid_for((size_t)g.ny * g.nx, 256, sms), 256, 0, s>>>(U, g, (size_t)nm * g.plane, gamma, prim);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mach(const double* U, const Grid& g, int nm, double gamma, double* mach, double* speed, int sms,
+                        cudaStream_t s) {
+    mach_kernel<<<grid_for((size_t)g.ny * g.nx, 256, sms), 256, 0, s>>>(U, g, (size_t)nm * g.plane, gamma, mach, speed);
     return cudaGetLastError();
 }
 

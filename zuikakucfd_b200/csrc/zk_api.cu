@@ -434,4 +434,20 @@ int zk_recover_primitives(zk_ctx* c, double* host_prim) {
     return ZK_OK;
 }
 
+int zk_mach_number(zk_ctx* c, double* host_mach, double* host_speed) {
+    if (int rc = check_ctx(c, true)) return rc;
+    if (!host_mach) return fail(ZK_ERR_ARG, "null argument");
+    ZK_CUDA(cudaSetDevice(c->opt.device));
+    double* mach = c->S2;
+    double* speed = c->S2 + c->g.plane;
+    ZK_CUDA(launch_mach(c->Un, c->g, c->nm, c->gamma, mach, speed, c->sms, c->stream));
+    ZK_CUDA(cudaMemcpy2DAsync(host_mach, sizeof(double) * c->g.nx, mach, sizeof(double) * c->g.pitch,
+                              sizeof(double) * c->g.nx, c->g.ny, cudaMemcpyDeviceToHost, c->stream));
+    if (host_speed)
+        ZK_CUDA(cudaMemcpy2DAsync(host_speed, sizeof(double) * c->g.nx, speed, sizeof(double) * c->g.pitch,
+                                  sizeof(double) * c->g.nx, c->g.ny, cudaMemcpyDeviceToHost, c->stream));
+    ZK_CUDA(cudaStreamSynchronize(c->stream));
+    return ZK_OK;
+}
+
 }  // extern "C"

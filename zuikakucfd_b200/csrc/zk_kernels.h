@@ -22,5 +22,7 @@ cudaError_t launch_max_speed_dg(const double* dof, const int8_t* kind, const Gri
                                 cudaStream_t s);
 cudaError_t launch_recover(const double* U, const Grid& g, int nm, double gamma, double* prim,
                            int sms, cudaStream_t s);
+cudaError_t launch_mach(const double* U, const Grid& g, int nm, double gamma, double* mach, double* speed, int sms,
+                        cudaStream_t s);
 
 }  // namespace zk

@@ -345,3 +345,70 @@ def saveMeshData(mesh: Mesh, rank: int, folder: str | os.PathLike) -> None:
     d.mkdir(parents=True, exist_ok=True)
     for c, name in enumerate(("U0", "U1", "U2", "U3")):
         np.savetxt(d / f"{name}_{rank}.dat", mesh._cons(c), fmt="%.6g")
+
+
+# ---- checkpoints and post-processing -------------------------------------------
+
+def saveCheckpoint(mesh: Mesh, path: str | os.PathLike, t: float = 0.0, step: int = 0) -> Path:
+    """Full-precision binary checkpoint of a Mesh: the whole conserved state
+    (all DG modes, ghosts included, FP64 bit for bit), bctype, grid, gamma,
+    the solver options, and the simulated time and step.  The reference only
+    writes text snapshots of the cell averages (saveMeshData,
+    src_WENO/fluid.cpp:558-577), from which a DG run cannot restart."""
+    p = Path(path)
+    if p.suffix != ".npz":
+        p = p.with_suffix(".npz")
+    np.savez(p, state=mesh.state, bctype=np.asarray(mesh.bctype, np.int32), grid=np.array([mesh.ny, mesh.nx]),
+             da=mesh.da, gamma=mesh.gamma, t=t, step=step,
+             options=np.array([f"{k}={v}" for k, v in mesh._opts.items()]))
+    return p
+
+
+def loadCheckpoint(path: str | os.PathLike, **overrides) -> tuple[Mesh, float, int]:
+    """(mesh, t, step) from saveCheckpoint; keyword overrides replace saved
+    options (e.g. precision="mixed" to continue a run on the fast path)."""
+    z = np.load(Path(path), allow_pickle=False)
+    opts = {}
+    for item in z["options"]:
+        k, v = str(item).split("=", 1)
+        opts[k] = int(v) if k in ("order", "device") else float(v) if k == "tvb_M" else v
+    opts.update(overrides)
+    ny, nx = (int(x) for x in z["grid"])
+    m = Mesh(ny, nx, float(z["da"]), float(z["gamma"]), **opts)
+    m.bctype = z["bctype"].astype(np.int32)
+    m.state = z["state"]
+    return m, float(z["t"]), int(z["step"])
+
+
+def computeMach(mesh: Mesh) -> tuple[np.ndarray, np.ndarray]:
+    """(Mach, |u|) of the cell averages, the plot notebook's compute_mach
+    (plot.ipynb cell 0), evaluated on the GPU from the device state."""
+    import ctypes as C
+    s = mesh.solver()
+    mach = np.empty((mesh.ny, mesh.nx))
+    speed = np.empty((mesh.ny, mesh.nx))
+    N.check(N.lib().zk_mach_number(s._h, N.dptr(mach), N.dptr(speed)))
+    return mach, speed
+
+
+def combineRankSnapshots(folder: str | os.PathLike, n_ranks: int, ghost: int = 3) -> np.ndarray:
+    """U[4][ny][nx] of a run the reference wrote as per-rank x-slabs
+    (U<c>_<rank>.dat), with each slab's exchange columns dropped: the first
+    slab keeps its left ring, the last its right ring (plot.ipynb
+    load_and_combine_data)."""
+    d = Path(folder)
+    out = []
+    for c in range(4):
+        parts = []
+        for r in range(n_ranks):
+            a = np.loadtxt(d / f"U{c}_{r}.dat", ndmin=2)
+            if n_ranks == 1:
+                parts.append(a)
+            elif r == 0:
+                parts.append(a[:, :-ghost])
+            elif r == n_ranks - 1:
+                parts.append(a[:, ghost:])
+            else:
+                parts.append(a[:, ghost:-ghost])
+        out.append(np.concatenate(parts, axis=1))
+    return np.stack(out)
