@@ -152,10 +152,13 @@ def dist_setup(n_gpus: int):
 
 
 def allreduce_max(pg, x: float) -> float:
+    """Max over ranks (the slowest rank's time); a device tensor under NCCL,
+    a host tensor under gloo."""
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
