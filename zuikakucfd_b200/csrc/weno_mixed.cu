@@ -62,6 +62,53 @@ __device__ __forceinline__ void weno5(T UL2, T UL1, T UP, T UR1, T UR2, T UR3, T
     UR = (e0 * qR0 + e1 * qR1 + e2 * qR2) / (e0 + e1 + e2);
 }
 
+// Packed FP32 pairs (sm_100 add/mul/fma .f32x2): one instruction issues the
+// same operation for two conserved variables.  Each lane rounds exactly as the
+// scalar instruction does; reciprocals stay per lane (MUFU has no pair form).
+__device__ __forceinline__ float2 f2(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+
+// weno5 above for two variables at once.  The ideal weights are scaled by 10
+// (1, 6, 3), which the normalisation divides out.
+__device__ __forceinline__ void weno5x2(float2 UL2, float2 UL1, float2 UP, float2 UR1, float2 UR2, float2 UR3,
+                                        float2& UL, float2& UR) {
+    const float2 eps = f2(1e-6f), C1 = f2(13.0f / 12.0f), C2 = f2(0.25f);
+    const float2 c13 = f2(1.0f / 3.0f), m76 = f2(-7.0f / 6.0f), c116 = f2(11.0f / 6.0f), m16 = f2(-1.0f / 6.0f),
+                 c56 = f2(5.0f / 6.0f);
+    const float2 m1 = f2(-1.0f), m2 = f2(-2.0f), m4 = f2(-4.0f), c3 = f2(3.0f), c6 = f2(6.0f);
+    const float2 qL0 = fma2(c116, UP, fma2(m76, UL1, mul2(c13, UL2)));
+    const float2 qL1 = fma2(c13, UR1, fma2(c56, UP, mul2(m16, UL1)));
+    const float2 qL2 = fma2(m16, UR2, fma2(c56, UR1, mul2(c13, UP)));
+    const float2 d0 = add2(fma2(m2, UL1, UL2), UP), d1 = fma2(c3, UP, fma2(m4, UL1, UL2));
+    const float2 d2 = add2(fma2(m2, UP, UL1), UR1), d3 = fma2(m1, UR1, UL1);
+    const float2 d4 = add2(fma2(m2, UR1, UP), UR2), d5 = add2(fma2(m4, UR1, mul2(c3, UP)), UR2);
+    const float2 t0 = add2(eps, fma2(mul2(C1, d0), d0, mul2(mul2(C2, d1), d1)));
+    const float2 t1 = add2(eps, fma2(mul2(C1, d2), d2, mul2(mul2(C2, d3), d3)));
+    const float2 t2 = add2(eps, fma2(mul2(C1, d4), d4, mul2(mul2(C2, d5), d5)));
+    {
+        const float2 a0 = rcp2(mul2(t0, t0)), a1 = mul2(c6, rcp2(mul2(t1, t1))), a2 = mul2(c3, rcp2(mul2(t2, t2)));
+        const float2 num = fma2(a2, qL2, fma2(a1, qL1, mul2(a0, qL0)));
+        UL = mul2(num, rcp2(add2(add2(a0, a1), a2)));
+    }
+    const float2 qR0 = fma2(c13, UR3, fma2(m76, UR2, mul2(c116, UR1)));
+    const float2 r0 = add2(fma2(m2, UR2, UR1), UR3), r1 = fma2(c3, UR1, fma2(m4, UR2, UR3));
+    const float2 r3 = fma2(m1, UR2, UP), r5 = fma2(c3, UR1, fma2(m4, UP, UL1));
+    const float2 s0 = add2(eps, fma2(mul2(C1, r0), r0, mul2(mul2(C2, r1), r1)));
+    const float2 s1 = add2(eps, fma2(mul2(C1, d4), d4, mul2(mul2(C2, r3), r3)));  // r2 == d4
+    const float2 s2 = add2(eps, fma2(mul2(C1, d2), d2, mul2(mul2(C2, r5), r5)));  // r4 == d2
+    const float2 e0 = rcp2(mul2(s0, s0)), e1 = mul2(c6, rcp2(mul2(s1, s1))), e2 = mul2(c3, rcp2(mul2(s2, s2)));
+    const float2 num = fma2(e2, qL1, fma2(e1, qL2, mul2(e0, qR0)));  // qR1 == qL2, qR2 == qL1
+    UR = mul2(num, rcp2(add2(add2(e0, e1), e2)));
+}
+
 // std::min / std::max argument order of the reference, for either precision.
 template <typename T>
 __device__ __forceinline__ T tmin(T a, T b) { return (b < a) ? b : a; }
@@ -133,7 +180,7 @@ struct MixedArgs {
 template <int TY>
 struct Smem {
     double stg[4][TY + 6][SX];  // TMA destination, FP64, ghosts fixed up in place (offset 0: 128-byte aligned)
-    float sU[4][TY + 6][HX];    // FP32 copy of the tile + halo
+    float2 sU[2][TY + 6][HX];   // FP32 copy of the tile + halo, pairs (rho, m_x) and (m_y, E)
     double sFx[4][TY][TX + 1];
     double sFy[4][TY + 1][TX];
     uint8_t sK[TY + 6][HX];     // kind | HIGH_MACH
@@ -146,7 +193,7 @@ template <bool XDIR, int TY>
 __device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamma, float gf) {
     constexpr int SU = XDIR ? 1 : HX;  // stride between stencil cells in sU / sK
     constexpr int SG = XDIR ? 1 : SX;  // and in stg
-    const float* u0 = XDIR ? &S.sU[0][r + 3][c] : &S.sU[0][r][c + 3];
+    const float2* u0 = XDIR ? &S.sU[0][r + 3][c] : &S.sU[0][r][c + 3];
     const uint8_t* k0 = XDIR ? &S.sK[r + 3][c] : &S.sK[r][c + 3];
     constexpr int PU = (TY + 6) * HX;  // plane stride of sU
     uint8_t hm = 0;
@@ -168,16 +215,16 @@ __device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamm
         }
         hllc<double>(QL, QR, gamma, F);
     } else {
-        float QL[4], QR[4], Ff[4];
+        float2 L[2], R[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float* u = u0 + q * PU;
-            weno5<float>(u[0], u[SU], u[2 * SU], u[3 * SU], u[4 * SU], u[5 * SU], QL[q], QR[q]);
+        for (int h = 0; h < 2; ++h) {
+            const float2* u = u0 + h * PU;
+            weno5x2(u[0], u[SU], u[2 * SU], u[3 * SU], u[4 * SU], u[5 * SU], L[h], R[h]);
         }
-        if (!XDIR) {
-            float t = QL[1]; QL[1] = QL[2]; QL[2] = t;
-            t = QR[1]; QR[1] = QR[2]; QR[2] = t;
-        }
+        // normal momentum into slot 1
+        float QL[4] = {L[0].x, XDIR ? L[0].y : L[1].x, XDIR ? L[1].x : L[0].y, L[1].y};
+        float QR[4] = {R[0].x, XDIR ? R[0].y : R[1].x, XDIR ? R[1].x : R[0].y, R[1].y};
+        float Ff[4];
         hllc<float>(QL, QR, gf, Ff);
 #pragma unroll
         for (int q = 0; q < 4; ++q) F[q] = (double)Ff[q];
@@ -259,8 +306,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
             const double prho = gm1 * (v[3] * v[0] - 0.5 * (v[1] * v[1] + v[2] * v[2]));
             if (!(v[0] > 0.0) || !(prho > 0.0) || v[3] * v[0] > 100.0 * prho) kd |= HIGH_MACH;
         }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) sU[q][r][c] = (float)v[q];
+        sU[0][r][c] = make_float2((float)v[0], (float)v[1]);
+        sU[1][r][c] = make_float2((float)v[2], (float)v[3]);
         sK[r][c] = kd;
     }
     __syncthreads();
