@@ -219,6 +219,8 @@ typedef struct zk_batch_options {
     int graph_steps;      /* RK steps per captured graph (1..1000; default 10)     */
     int autotune;         /* 0 off, 1 on (cached per process), 2 re-tune           */
     size_t arena_bytes;   /* > 0: one device allocation all problems carve from    */
+    int weno_variant;     /* -1: tuned; 0..5: pin the WENO tile variant (the      */
+                          /* autotuner then tunes CTAs per SM only)               */
 } zk_batch_options;
 
 typedef struct zk_batch_report {
@@ -255,11 +257,16 @@ int zk_batch_problem_info(zk_batch* b, int id, zk_batch_problem* out);
 /* The dt of each step problem `id` took (n <= its step count). */
 int zk_batch_dt_history(zk_batch* b, int id, double* dts, int n);
 /* Chosen configuration of group g (groups form at zk_batch_run): tile variant
- * (index into the tile heights {4, 8} for WENO, {2, 4} for mixed DG) and CTAs
- * per SM of the stage kernel; *ngroups = number of groups.  Any pointer may be
- * NULL; g = -1 only reports the number of groups. */
+ * of the stage kernel (WENO: 3 * h + k, tile height {4, 8}[h] worked by
+ * {rows/2 + 1, rows + 1, 2 rows + 2}[k] warps; mixed DG: index into the tile
+ * heights {2, 4}) and its CTAs per SM; *ngroups = number of groups.  Any
+ * pointer may be NULL; g = -1 only reports the number of groups. */
 int zk_batch_group_config(zk_batch* b, int g, int* method, int* precision, int* order, int* variant,
                           int* ctas_per_sm, int* ngroups);
+/* Tile of group g's stage kernel: cells per tile (tile_rows x tile_cols) and
+ * the threads that work one tile, so threads per cell = threads_per_tile /
+ * (tile_rows * tile_cols).  Any pointer may be NULL. */
+int zk_batch_group_tile(zk_batch* b, int g, int* tile_rows, int* tile_cols, int* threads_per_tile);
 void zk_batch_destroy(zk_batch* b);
 
 #ifdef __cplusplus

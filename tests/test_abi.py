@@ -53,3 +53,20 @@ def test_default_options_and_errors_without_device(lib):
     assert b"method" in lib.zk_last_error()
     assert lib.zk_create(None, C.byref(h)) == 1
     assert lib.zk_version() >= 100
+
+
+def test_batch_default_options_and_bad_options(lib):
+    """Batch defaults (tuned WENO tile, 10 graph steps) and option checks that
+    run before any device work."""
+    from zuikakucfd_b200._native import zk_batch_options
+    lib.zk_last_error.restype = C.c_char_p
+    o = zk_batch_options()
+    lib.zk_batch_default_options(C.byref(o))
+    assert (o.device, o.policy, o.graph_steps, o.autotune, o.arena_bytes, o.weno_variant) == (0, 0, 10, 1, 0, -1)
+    h = C.c_void_p()
+    for field, bad, word in (("weno_variant", 6, b"weno_variant"), ("graph_steps", 0, b"graph_steps"),
+                             ("autotune", 3, b"autotune"), ("policy", 9, b"policy")):
+        lib.zk_batch_default_options(C.byref(o))
+        setattr(o, field, bad)
+        assert lib.zk_batch_create(C.byref(o), C.byref(h)) == 1
+        assert word in lib.zk_last_error()

@@ -100,9 +100,30 @@ def test_batch_matches_single_problems(policy, active, gsteps):
         for g in groups:
             assert g["ctas_per_sm"] >= 1
             if g["method"] == "weno":
-                assert g["tile_rows"] in (4, 8)
+                r = g["tile_rows"]
+                assert r in (4, 8) and g["tile_cols"] == 32
+                assert g["threads_per_tile"] // 32 in (r // 2 + 1, r + 1, 2 * r + 2)
             elif g["precision"] == "mixed":
-                assert g["tile_rows"] in (2, 4)
+                assert g["tile_rows"] in (2, 4) and g["threads_per_cell"] == 1.0
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_batch_weno_tile_variants(variant):
+    """Every WENO tile variant (tile height x warps per tile, pinned instead
+    of tuned) gives the single-run states bit for bit."""
+    from zuikakucfd_b200.batch import Batch
+    specs = [s for s in _specs() if s["method"] == "weno"]
+    with Batch(policy="all", graph_steps=4, autotune=1, weno_variant=variant) as bt:
+        ids = [bt.add(**s) for s in specs]
+        rep = bt.run()
+        assert rep["done"] == len(specs)
+        for pid, spec in zip(ids, specs):
+            ref, _ = _single(spec, bt.dt_history(pid))
+            assert np.array_equal(bt.get_state(pid), ref), (variant, spec["precision"])
+        rows = (4, 8)[variant // 3]
+        for g in bt.groups():
+            assert g["variant"] == variant and g["tile_rows"] == rows
+            assert g["threads_per_tile"] == 32 * (rows // 2 + 1, rows + 1, 2 * rows + 2)[variant % 3]
 
 
 def test_batch_failure_stays_local():
@@ -142,3 +163,5 @@ def test_batch_rejects_bad_input():
             bt.add(c.bctype, c.da, c.gamma, c.conserved(), 5, -1.0)
         with pytest.raises(ZkError, match="ZK_ERR_STATE"):
             bt.run()  # empty batch
+    with pytest.raises(ZkError, match="ZK_ERR_ARG"):
+        Batch(weno_variant=6)

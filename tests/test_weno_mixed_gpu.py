@@ -95,3 +95,19 @@ def test_high_mach_jet_positivity_and_fp64_faces():
     assert s64 == 0 and smx == 0
     for q in range(4):
         assert rel_l1(mix[q], f64[q]) < 1e-6, q
+
+
+def test_centre_detonation_large_magnitudes():
+    """The generator notebook's centre detonation (p = 1e10 Pa in a 5-cell
+    charge, E ~ 2.5e10): conserved values beyond the FP32 range of the WENO
+    smoothness indicators make their faces FP64, so the mixed path stays
+    finite and positive and close to the FP64 path through the blast."""
+    from zuikakucfd_b200 import cases
+    c = cases.center_detonation(128, domain=256.0)
+    dt = cases.cfl_dt(c, 0.4)
+    f64, s64 = run(c, dt, 30, "fp64")
+    mix, smx = run(c, dt, 30, "mixed")
+    assert s64 == 0 and smx == 0
+    assert np.isfinite(mix).all()
+    for q in range(4):
+        assert rel_l1(mix[q], f64[q]) < 1e-6, q

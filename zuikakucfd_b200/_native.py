@@ -40,7 +40,8 @@ class zk_options(C.Structure):
 
 class zk_batch_options(C.Structure):
     _fields_ = [("device", C.c_int), ("policy", C.c_int), ("active_cells", C.c_double),
-                ("graph_steps", C.c_int), ("autotune", C.c_int), ("arena_bytes", C.c_size_t)]
+                ("graph_steps", C.c_int), ("autotune", C.c_int), ("arena_bytes", C.c_size_t),
+                ("weno_variant", C.c_int)]
 
 
 class zk_batch_report(C.Structure):
@@ -110,6 +111,7 @@ _SIGS = {
     "zk_batch_problem_info": (C.c_int, [_P, C.c_int, C.POINTER(zk_batch_problem)]),
     "zk_batch_dt_history": (C.c_int, [_P, C.c_int, _D, C.c_int]),
     "zk_batch_group_config": (C.c_int, [_P, C.c_int] + [C.POINTER(C.c_int)] * 6),
+    "zk_batch_group_tile": (C.c_int, [_P, C.c_int] + [C.POINTER(C.c_int)] * 3),
     "zk_batch_destroy": (None, [_P]),
 }
 

@@ -24,7 +24,7 @@ from . import cases
 
 class Batch:
     def __init__(self, policy: str = "all", active_cells: float = 8e6, graph_steps: int = 10,
-                 autotune: int = 1, arena_bytes: int = 0, device: int = 0):
+                 autotune: int = 1, arena_bytes: int = 0, device: int = 0, weno_variant: int = -1):
         L = N.lib()
         o = N.zk_batch_options()
         L.zk_batch_default_options(C.byref(o))
@@ -34,6 +34,7 @@ class Batch:
         o.graph_steps = int(graph_steps)
         o.autotune = int(autotune)
         o.arena_bytes = int(arena_bytes)
+        o.weno_variant = int(weno_variant)
         h = C.c_void_p()
         N.check(L.zk_batch_create(C.byref(o), C.byref(h)))
         self._h = h
@@ -114,8 +115,9 @@ class Batch:
         return out
 
     def groups(self) -> list[dict]:
-        """Per problem group: method, precision, order and the chosen tile
-        height / CTAs per SM of its stage kernel."""
+        """Per problem group: method, precision, order, the tile the autotuner
+        chose for its stage kernel (cells per tile, threads per tile and per
+        cell) and its CTAs per SM."""
         L = N.lib()
         ng = C.c_int()
         N.check(L.zk_batch_group_config(self._h, -1, None, None, None, None, None, C.byref(ng)))
@@ -126,11 +128,12 @@ class Batch:
             v = [C.c_int() for _ in range(5)]
             N.check(L.zk_batch_group_config(self._h, g, *[C.byref(x) for x in v], None))
             m, p, o, var, ctas = (x.value for x in v)
-            rows = ({0: 4, 1: 8} if m == 0 else {0: 2, 1: 4}).get(var)
-            if m == 1 and p == 0:
-                rows = None  # FP64 DG passes run over row segments
-            out.append({"method": inv_m[m], "precision": inv_p[p], "order": o, "tile_rows": rows,
-                        "ctas_per_sm": ctas})
+            t = [C.c_int() for _ in range(3)]
+            N.check(L.zk_batch_group_tile(self._h, g, *[C.byref(x) for x in t]))
+            rows, cols, threads = (x.value for x in t)
+            out.append({"method": inv_m[m], "precision": inv_p[p], "order": o, "variant": var,
+                        "tile_rows": rows, "tile_cols": cols, "threads_per_tile": threads,
+                        "threads_per_cell": threads / (rows * cols), "ctas_per_sm": ctas})
         return out
 
 

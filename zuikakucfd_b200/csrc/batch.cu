@@ -104,7 +104,7 @@ struct BGroup {
     int* d_members = nullptr;
     int* d_dir[NDIR] = {nullptr, nullptr, nullptr};
     int cap = 0;
-    int variant = 1;    // tile variant of the stage kernel
+    int variant = 1;    // tile variant of the stage kernel (batch.cuh)
     int ctas = 0;       // CTAs per SM of the stage kernel
     int ctas_cell = 0;  // FP64 DG cell pass
     double tune_ms = 0.0;
@@ -170,7 +170,7 @@ int balloc_t(zk_batch* b, T** p, size_t count) {
 // Tiles of problem p in tiling d of its group (tile variant v).
 int tiles_of(const BGroup& g, const BProblem& p, int d, int v) {
     if (d == DIR_RED) return batch_red_tiles(p.ny, p.nx);
-    if (!g.dg()) return ((p.nx + 31) / 32) * ((p.ny + kWenoTileRows[v] - 1) / kWenoTileRows[v]);
+    if (!g.dg()) return ((p.nx + 31) / 32) * ((p.ny + weno_variant_rows(v) - 1) / weno_variant_rows(v));
     if (g.mixed()) return dg_mixed_batch_tiles(v, p.ny, p.nx);
     return dg_fp64_batch_tiles(d == DIR_STAGE ? 0 : 1, p.ny, p.nx);
 }
@@ -243,12 +243,14 @@ double stage_flops(const zk_options& o) {
 }
 
 // Time the tile variants x persistent grid sizes of group g's stage-1 kernel
-// on a sample of its problems (up to 8M updated cells); keep the fastest.
+// on a sample of its problems (up to 8M updated cells); keep the fastest.  A
+// pinned WENO variant is timed alone and its result is not cached.
 int autotune(zk_batch* b, BGroup& g) {
     int dev = 0;
     BK_CUDA(cudaGetDevice(&dev));
     const auto key = std::make_tuple(dev, g.method, g.precision, g.order);
-    if (b->opt.autotune == 1) {
+    const bool pinned = !g.dg() && b->opt.weno_variant >= 0;
+    if (b->opt.autotune == 1 && !pinned) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) {
@@ -268,11 +270,11 @@ int autotune(zk_batch* b, BGroup& g) {
     for (int s : sample) adm[g.members[s]] = 1;
     BK_CUDA(cudaMemcpyAsync(b->d_admitted, adm.data(), sizeof(int) * adm.size(), cudaMemcpyHostToDevice, b->stream));
     const bool fp64dg = g.dg() && !g.mixed();
-    const int nvar = fp64dg ? 1 : 2;
+    const int nvar = (fp64dg || pinned) ? 1 : g.dg() ? 2 : kWenoVariants;
     float best = 3.0e38f;
     int best_v = g.variant, best_c = g.ctas;
     for (int v = 0; v < nvar; ++v) {
-        const int var = fp64dg ? g.variant : v;
+        const int var = (fp64dg || pinned) ? g.variant : v;
         const int keep = g.variant;
         g.variant = var;
         const int rc = upload_dirs(b, g, sample);
@@ -307,6 +309,7 @@ int autotune(zk_batch* b, BGroup& g) {
                             b->stream));
     BK_CUDA(cudaMemsetAsync(b->d_admitted, 0, sizeof(int) * b->probs.size(), b->stream));
     BK_CUDA(cudaStreamSynchronize(b->stream));
+    if (pinned) return ZK_OK;
     std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune[key] = {g.variant, g.ctas};
     return ZK_OK;
@@ -466,7 +469,7 @@ int finalize(zk_batch* b) {
                                     b->stream));
             BK_CUDA(cudaStreamSynchronize(b->stream));
         }
-        g.variant = 1;
+        g.variant = g.dg() ? 1 : b->opt.weno_variant >= 0 ? b->opt.weno_variant : kWenoDefaultVariant;
         g.ctas = occupancy(g, g.variant);
         if (g.dg() && !g.mixed()) g.ctas_cell = dg_fp64_batch_occupancy(g.order, 1);
         if (g.ctas <= 0) return bfail(ZK_ERR_CUDA, "stage kernel of group %d cannot be resident", (int)gi);
@@ -492,6 +495,7 @@ void zk_batch_default_options(zk_batch_options* o) {
     o->graph_steps = 10;
     o->autotune = 1;
     o->arena_bytes = 0;
+    o->weno_variant = -1;
 }
 
 int zk_batch_create(const zk_batch_options* o, zk_batch** out) {
@@ -500,6 +504,8 @@ int zk_batch_create(const zk_batch_options* o, zk_batch** out) {
     if (o->policy != ZK_BATCH_ALL && o->policy != ZK_BATCH_SJF) return bfail(ZK_ERR_ARG, "unknown policy %d", o->policy);
     if (o->graph_steps < 1 || o->graph_steps > 1000) return bfail(ZK_ERR_ARG, "graph_steps must be 1..1000");
     if (o->autotune < 0 || o->autotune > 2) return bfail(ZK_ERR_ARG, "autotune must be 0, 1 or 2");
+    if (o->weno_variant < -1 || o->weno_variant >= kWenoVariants)
+        return bfail(ZK_ERR_ARG, "weno_variant must be -1 or 0..%d", kWenoVariants - 1);
     BK_CUDA(cudaSetDevice(o->device));
     zk_batch* b = new zk_batch();
     b->opt = *o;
@@ -776,6 +782,27 @@ int zk_batch_group_config(zk_batch* b, int g, int* method, int* precision, int* 
     if (order) *order = G.order;
     if (variant) *variant = G.variant;
     if (ctas_per_sm) *ctas_per_sm = G.ctas;
+    return ZK_OK;
+}
+
+int zk_batch_group_tile(zk_batch* b, int g, int* tile_rows, int* tile_cols, int* threads_per_tile) {
+    if (!b) return bfail(ZK_ERR_ARG, "null batch");
+    if (g < 0 || g >= (int)b->groups.size()) return bfail(ZK_ERR_ARG, "no group %d (groups form at zk_batch_run)", g);
+    const BGroup& G = b->groups[g];
+    int rows = 1, cols = 32, threads = 32;
+    if (!G.dg()) {
+        rows = weno_variant_rows(G.variant);
+        threads = 32 * weno_variant_warps(G.variant);
+    } else if (G.mixed()) {
+        rows = kDgTileRows[G.variant];
+        threads = rows * cols;
+    } else {
+        cols = kDgCellBlock;  // the FP64 DG cell pass
+        threads = cols;
+    }
+    if (tile_rows) *tile_rows = rows;
+    if (tile_cols) *tile_cols = cols;
+    if (threads_per_tile) *threads_per_tile = threads;
     return ZK_OK;
 }
 

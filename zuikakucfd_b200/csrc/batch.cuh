@@ -39,13 +39,37 @@ struct BatchCtl {
     int lam_ready;              // lam already holds the current state's speed (stage-3 epilogue)
 };
 
-// Tile heights of the WENO stage kernels the autotuner chooses between.
+// Tile variants of the WENO stage kernels the autotuner chooses between:
+// v = 3 * h + k is a 32 x kWenoTileRows[h] tile worked by weno_tile_warps
+// warps.  A tile has 2 rows + 2 face-row tasks (rows + 1 of x faces, rows + 1
+// of y faces); k = 0, 1, 2 give each warp about four, two or one of them, so
+// threads per cell is about 0.6, 1.2 or 2.4: fewer threads leave each more
+// registers, more threads hide more latency per resident tile.
 constexpr int kWenoTileRows[2] = {4, 8};
-// Tile heights of the mixed-precision DG stage kernel.
+constexpr int kWenoVariants = 6;
+constexpr int weno_tile_warps(int rows, int k) { return k == 0 ? rows / 2 + 1 : k == 1 ? rows + 1 : 2 * rows + 2; }
+constexpr int weno_variant_rows(int v) { return kWenoTileRows[v / 3]; }
+constexpr int weno_variant_warps(int v) { return weno_tile_warps(kWenoTileRows[v / 3], v % 3); }
+constexpr int kWenoDefaultVariant = 4;  // 32 x 8, 9 warps
+// Tile heights of the mixed-precision DG stage kernel (one thread per cell).
 constexpr int kDgTileRows[2] = {2, 4};
+// Row segment of the FP64 DG cell pass (one thread per cell).
+constexpr int kDgCellBlock = 64;
 
-// One WENO problem of a group.  tmap[v][b]: TMA map over buffer b (U^n,
-// stage 1, stage 2) with the box of tile variant v (mixed precision only).
+// CTAs per SM to promise in __launch_bounds__ for a persistent stage kernel:
+// as many as keep every thread within the register share of `thread_budget`
+// threads per SM and as many as the SM's 228 KB of shared memory holds (with
+// the 1 KB each resident CTA reserves).
+constexpr int batch_min_blocks(int nthread, int thread_budget, unsigned long smem) {
+    const int by_regs = thread_budget / nthread;
+    const int by_smem = (int)(233472ul / (smem + 1024ul + 512ul));
+    const int b = by_regs < by_smem ? by_regs : by_smem;
+    return b < 1 ? 1 : b;
+}
+
+// One WENO problem of a group.  tmap[h][b]: TMA map over buffer b (U^n,
+// stage 1, stage 2) with the box of tile height kWenoTileRows[h] (mixed
+// precision only).
 struct alignas(64) WenoItem {
     CUtensorMap tmap[2][3];
     double* U[3];

@@ -401,7 +401,7 @@ __device__ __forceinline__ void limit_cell(double (&o)[4][(P + 1) * (P + 1)], bo
     }
 }
 
-constexpr int kCellBlock = 64;
+constexpr int kCellBlock = kDgCellBlock;
 
 // Cells (i, jb + threadIdx.x); sd[v][threadIdx.x] is this thread's (filled)
 // stage input, column-private.  Returns the cell's max corner wave speed when

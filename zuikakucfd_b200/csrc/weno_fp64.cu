@@ -19,12 +19,12 @@
 namespace zk {
 namespace {
 
-// A tile is 32 x TY cells; TY + 1 warps take the 2 TY + 2 face-row tasks
-// (TY + 1 x-face rows, TY + 1 y-face rows) in two rounds.
+// A tile is 32 x TY cells; NW warps (TY + 1 by default) take the 2 TY + 2
+// face-row tasks (TY + 1 x-face rows, TY + 1 y-face rows) in turn.
 constexpr int TX = 32, HX = TX + 6;
-template <int TY>
+template <int TY, int NW = TY + 1>
 struct Tile {
-    static constexpr int HY = TY + 6, NWARP = TY + 1, NTHREAD = NWARP * 32;
+    static constexpr int HY = TY + 6, NWARP = NW, NTHREAD = NW * 32;
 };
 
 // weno5_reconstruct, src_WENO/fluid.cpp:230-263
@@ -125,9 +125,9 @@ struct Smem {
 // One tile whose top-left cell is (i0, j0).  Ends with every thread past its
 // last shared-memory read, so a persistent caller may reuse S after a barrier.
 // Returns the thread's max wave speed of the cells it wrote (want_lam), else 0.
-template <int TY>
+template <int TY, int NW = TY + 1>
 __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0, Smem<TY>& S) {
-    constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
+    constexpr int HY = Tile<TY, NW>::HY, NWARP = Tile<TY, NW>::NWARP, NTHREAD = Tile<TY, NW>::NTHREAD;
     auto& sU = S.sU;
     auto& sFx = S.sFx;
     auto& sFy = S.sFy;
@@ -248,8 +248,10 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 3) weno_stage_fp64_kernel(St
 // global tiles b, b + gridDim.x, ...; stage s reads U[s-1] (U^n at stage 1)
 // and writes U[s % 3].  Stage 3 also leaves the max wave speed of the new
 // state (computeMaxSpeed over all cells) in the problem's control block.
-template <int TY>
-__global__ void __launch_bounds__(Tile<TY>::NTHREAD, 864 / Tile<TY>::NTHREAD)
+// Tile variant V (batch.cuh); the register share is that of 864 threads per
+// SM (72 registers).
+template <int V, int TY = weno_variant_rows(V), int NW = weno_variant_warps(V)>
+__global__ void __launch_bounds__(NW * 32, batch_min_blocks(NW * 32, 864, sizeof(Smem<TY>)))
     weno_stage_fp64_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
                                  int stage) {
     __shared__ Smem<TY> S;
@@ -275,7 +277,7 @@ __global__ void __launch_bounds__(Tile<TY>::NTHREAD, 864 / Tile<TY>::NTHREAD)
         }
         __syncthreads();
         if (s_org[2]) {
-            const double m = stage_tile<TY>(sa, s_org[0], s_org[1], S);
+            const double m = stage_tile<TY, NW>(sa, s_org[0], s_org[1], S);
             if (stage == 3) block_max_commit_to(m, s_lam);  // the next step's wave speed
         }
         __syncthreads();
@@ -284,24 +286,44 @@ __global__ void __launch_bounds__(Tile<TY>::NTHREAD, 864 / Tile<TY>::NTHREAD)
 
 }  // namespace
 
+namespace {
+template <int V>
+cudaError_t launch_batch_v(const WenoItem* items, const int* dir, int cap, int stage, int grid, cudaStream_t s) {
+    weno_stage_fp64_batch_kernel<V><<<grid, weno_variant_warps(V) * 32, 0, s>>>(items, dir, cap, stage);
+    return cudaGetLastError();
+}
+template <int V>
+int occupancy_v() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_fp64_batch_kernel<V>, weno_variant_warps(V) * 32, 0);
+    return n;
+}
+}  // namespace
+
 cudaError_t launch_weno_stage_fp64_batch(int variant, const WenoItem* items, const int* dir, int cap, int stage,
                                          int grid, cudaStream_t s) {
-    if (variant == 0)
-        weno_stage_fp64_batch_kernel<kWenoTileRows[0]><<<grid, Tile<kWenoTileRows[0]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
-    else
-        weno_stage_fp64_batch_kernel<kWenoTileRows[1]><<<grid, Tile<kWenoTileRows[1]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
-    return cudaGetLastError();
+    static_assert(kWenoVariants == 6, "one case per tile variant");
+    switch (variant) {
+        case 0: return launch_batch_v<0>(items, dir, cap, stage, grid, s);
+        case 1: return launch_batch_v<1>(items, dir, cap, stage, grid, s);
+        case 2: return launch_batch_v<2>(items, dir, cap, stage, grid, s);
+        case 3: return launch_batch_v<3>(items, dir, cap, stage, grid, s);
+        case 4: return launch_batch_v<4>(items, dir, cap, stage, grid, s);
+        case 5: return launch_batch_v<5>(items, dir, cap, stage, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 int weno_fp64_batch_occupancy(int variant) {
-    int n = 0;
-    if (variant == 0)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_fp64_batch_kernel<kWenoTileRows[0]>,
-                                                      Tile<kWenoTileRows[0]>::NTHREAD, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_fp64_batch_kernel<kWenoTileRows[1]>,
-                                                      Tile<kWenoTileRows[1]>::NTHREAD, 0);
-    return n;
+    switch (variant) {
+        case 0: return occupancy_v<0>();
+        case 1: return occupancy_v<1>();
+        case 2: return occupancy_v<2>();
+        case 3: return occupancy_v<3>();
+        case 4: return occupancy_v<4>();
+        case 5: return occupancy_v<5>();
+        default: return 0;
+    }
 }
 
 cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,

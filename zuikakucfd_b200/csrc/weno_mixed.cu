@@ -4,9 +4,12 @@
 //   * reconstruction and HLLC fluxes in FP32 (this file is compiled with
 //     --use_fast_math: FP32 division and square root map to the MUFU
 //     approximations; FP64 arithmetic is unaffected);
-//   * faces whose 6-cell stencil touches a high-Mach cell -- E > 100 p, where
-//     recovering p = (gamma-1)(E - |m|^2 / 2 rho) from FP32 values would lose
-//     more than two of its digits to cancellation -- are evaluated in FP64;
+//   * faces whose 6-cell stencil touches an FP64 cell are evaluated in FP64.
+//     A cell is FP64 when it is high-Mach -- E > 100 p, where recovering
+//     p = (gamma-1)(E - |m|^2 / 2 rho) from FP32 values would lose more than
+//     two of its digits to cancellation -- or when a conserved value reaches
+//     kFp32Max, beyond which the FP32 smoothness indicators (t ~ 33 |U|^2)
+//     square past the range of the reciprocal and the weights turn to 0/0;
 //   * interface fluxes are kept in FP64 in shared memory, and dU and the
 //     Shu-Osher combine are FP64: the conserved state is accumulated in FP64;
 //   * the positivity check recovers p from the FP64 result.
@@ -24,14 +27,16 @@
 namespace zk {
 namespace {
 
-// A tile is 32 x TY cells; TY + 1 warps take the 2 TY + 2 face-row tasks.
+// A tile is 32 x TY cells; NW warps (TY + 1 by default) take the 2 TY + 2
+// face-row tasks in turn.
 constexpr int TX = 32, HX = TX + 6;
 constexpr int SX = TX + 8;  // staged columns: x from j0-4 (16-byte aligned) to j0+35
-template <int TY>
+template <int TY, int NW = TY + 1>
 struct Tile {
-    static constexpr int HY = TY + 6, NWARP = TY + 1, NTHREAD = NWARP * 32;
+    static constexpr int HY = TY + 6, NWARP = NW, NTHREAD = NW * 32;
 };
-constexpr uint8_t HIGH_MACH = 0x10;
+constexpr uint8_t FP64_CELL = 0x10;
+constexpr double kFp32Max = 1e8;  // t^2 <= (33.4 kFp32Max^2)^2 ~ 1e35 < 2^126
 
 // weno5_reconstruct (src_WENO/fluid.cpp:230-263), any precision.
 template <typename T>
@@ -183,12 +188,12 @@ struct Smem {
     float2 sU[2][TY + 6][HX];   // FP32 copy of the tile + halo, pairs (rho, m_x) and (m_y, E)
     double sFx[4][TY][TX + 1];
     double sFy[4][TY + 1][TX];
-    uint8_t sK[TY + 6][HX];     // kind | HIGH_MACH
+    uint8_t sK[TY + 6][HX];     // kind | FP64_CELL
 };
 
 // Flux of one face: XDIR, the x face left of tile cell (r, c) (stencil cells
 // (r, c-3 .. c+2)); else the y face above it (cells (r-3 .. r+2, c), normal
-// momentum swapped into slot 1).  FP32 unless a stencil cell is high-Mach.
+// momentum swapped into slot 1).  FP32 unless a stencil cell is FP64_CELL.
 template <bool XDIR, int TY>
 __device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamma, float gf) {
     constexpr int SU = XDIR ? 1 : HX;  // stride between stencil cells in sU / sK
@@ -200,7 +205,7 @@ __device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamm
 #pragma unroll
     for (int n = 0; n < 6; ++n) hm |= k0[n * SU];
     double F[4];
-    if (hm & HIGH_MACH) {
+    if (hm & FP64_CELL) {
         const double* g0 = XDIR ? &S.stg[0][r + 3][c + 1] : &S.stg[0][r][c + 4];
         constexpr int PG = (TY + 6) * SX;
         double QL[4], QR[4];
@@ -243,11 +248,11 @@ __device__ __forceinline__ void face_flux(Smem<TY>& S, int r, int c, double gamm
 // STATUS_TIMEOUT) when the TMA copy did not land within the spin limit.
 // Every thread is past its last shared-memory access on return.  umax: the
 // thread's max wave speed of the cells it wrote (want_lam), else 0.
-template <int TY>
+template <int TY, int NW = TY + 1>
 __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedArgs& a, int j0, int i0, Smem<TY>& S,
                                            uint64_t* bar, uint32_t phase, double& umax) {
     umax = 0.0;
-    constexpr int HY = Tile<TY>::HY, NWARP = Tile<TY>::NWARP, NTHREAD = Tile<TY>::NTHREAD;
+    constexpr int HY = Tile<TY, NW>::HY, NWARP = Tile<TY, NW>::NWARP, NTHREAD = Tile<TY, NW>::NTHREAD;
     auto& stg = S.stg;
     auto& sU = S.sU;
     auto& sFx = S.sFx;
@@ -281,7 +286,7 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
                                                           16 * half));
     }
 
-    // 2. ghost fill from the source map, FP32 copy, high-Mach flags
+    // 2. ghost fill from the source map, FP32 copy, FP64_CELL flags
     const double gm1 = a.gamma - 1.0;
     for (int t = threadIdx.x; t < HY * HX; t += NTHREAD) {
         const int r = t / HX, c = t - r * HX;
@@ -304,7 +309,9 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
             // high-Mach test E > 100 p, p = (gamma-1)(E - |m|^2 / 2 rho), with
             // both sides multiplied by rho > 0 (no division)
             const double prho = gm1 * (v[3] * v[0] - 0.5 * (v[1] * v[1] + v[2] * v[2]));
-            if (!(v[0] > 0.0) || !(prho > 0.0) || v[3] * v[0] > 100.0 * prho) kd |= HIGH_MACH;
+            // with rho > 0 and p > 0, |m| <= sqrt(2 rho E) <= rho + E bounds every component
+            if (!(v[0] > 0.0) || !(prho > 0.0) || v[3] * v[0] > 100.0 * prho || !(v[0] + v[3] < kFp32Max))
+                kd |= FP64_CELL;
         }
         sU[0][r][c] = make_float2((float)v[0], (float)v[1]);
         sU[1][r][c] = make_float2((float)v[2], (float)v[3]);
@@ -361,8 +368,8 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
         }
         if (upd) {
             if (isnan(o[0]) || isnan(o[1]) || isnan(o[2]) || isnan(o[3])) flags |= STATUS_NAN;
-            if (!(o[0] > 0.0)) flags |= STATUS_RHO;
-            else if (!(gm1 * (o[3] - 0.5 * (o[1] * o[1] + o[2] * o[2]) / o[0]) > 0.0)) flags |= STATUS_P;
+            if (!(o[0] > 0.0)) flags |= STATUS_RHO;  // then p > 0 <=> rho E > |m|^2 / 2
+            else if (!(o[3] * o[0] - 0.5 * (o[1] * o[1] + o[2] * o[2]) > 0.0)) flags |= STATUS_P;
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) a.Uout[q * plane + k] = o[q];
@@ -395,13 +402,13 @@ __global__ void __launch_bounds__(Tile<8>::NTHREAD, 5)
 }
 
 // Persistent stage over every listed problem of a batch group (tile variant
-// v: kWenoTileRows[v] rows).  The tensor maps live in the item array in
-// global memory, written by the host before the launch.
-template <int V>
-__global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1440 / Tile<kWenoTileRows[V]>::NTHREAD)
+// V of batch.cuh; the register share is that of 1440 threads per SM, 40
+// registers).  The tensor maps live in the item array in global memory,
+// written by the host before the launch.
+template <int V, int TY = weno_variant_rows(V), int NW = weno_variant_warps(V)>
+__global__ void __launch_bounds__(NW * 32, batch_min_blocks(NW * 32, 1440, sizeof(Smem<TY>)))
     weno_stage_mixed_batch_kernel(const WenoItem* __restrict__ items, const int* __restrict__ dir, int cap,
                                   int stage) {
-    constexpr int TY = kWenoTileRows[V];
     __shared__ __align__(128) Smem<TY> S;
     __shared__ __align__(8) uint64_t bar;
     __shared__ MixedArgs sa;  // the current tile's problem, kept out of registers
@@ -425,7 +432,7 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1440 / Tile<k
                 sa = MixedArgs{it.U[stage - 1], it.U[0], it.U[stage % 3], it.kind, it.gsrc, it.g,
                                ctl->dtdx, ctl->dtdy, it.gamma, stage, &ctl->status, stage == 3};
                 s_lam = &ctl->lam;
-                s_map = &it.tmap[V][stage - 1];
+                s_map = &it.tmap[V / 3][stage - 1];
                 asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(
                                  reinterpret_cast<uint64_t>(s_map))
                              : "memory");
@@ -434,7 +441,7 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1440 / Tile<k
         __syncthreads();
         if (s_org[2]) {
             double umax;
-            if (!stage_tile<TY>(s_map, sa, s_org[0], s_org[1], S, &bar, phase, umax)) return;
+            if (!stage_tile<TY, NW>(s_map, sa, s_org[0], s_org[1], S, &bar, phase, umax)) return;
             phase ^= 1u;
             if (stage == 3) block_max_commit_to(umax, s_lam);  // the next step's wave speed
         }
@@ -444,24 +451,44 @@ __global__ void __launch_bounds__(Tile<kWenoTileRows[V]>::NTHREAD, 1440 / Tile<k
 
 }  // namespace
 
+namespace {
+template <int V>
+cudaError_t launch_batch_v(const WenoItem* items, const int* dir, int cap, int stage, int grid, cudaStream_t s) {
+    weno_stage_mixed_batch_kernel<V><<<grid, weno_variant_warps(V) * 32, 0, s>>>(items, dir, cap, stage);
+    return cudaGetLastError();
+}
+template <int V>
+int occupancy_v() {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_mixed_batch_kernel<V>, weno_variant_warps(V) * 32, 0);
+    return n;
+}
+}  // namespace
+
 cudaError_t launch_weno_stage_mixed_batch(int variant, const WenoItem* items, const int* dir, int cap, int stage,
                                           int grid, cudaStream_t s) {
-    if (variant == 0)
-        weno_stage_mixed_batch_kernel<0><<<grid, Tile<kWenoTileRows[0]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
-    else
-        weno_stage_mixed_batch_kernel<1><<<grid, Tile<kWenoTileRows[1]>::NTHREAD, 0, s>>>(items, dir, cap, stage);
-    return cudaGetLastError();
+    static_assert(kWenoVariants == 6, "one case per tile variant");
+    switch (variant) {
+        case 0: return launch_batch_v<0>(items, dir, cap, stage, grid, s);
+        case 1: return launch_batch_v<1>(items, dir, cap, stage, grid, s);
+        case 2: return launch_batch_v<2>(items, dir, cap, stage, grid, s);
+        case 3: return launch_batch_v<3>(items, dir, cap, stage, grid, s);
+        case 4: return launch_batch_v<4>(items, dir, cap, stage, grid, s);
+        case 5: return launch_batch_v<5>(items, dir, cap, stage, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 int weno_mixed_batch_occupancy(int variant) {
-    int n = 0;
-    if (variant == 0)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_mixed_batch_kernel<0>,
-                                                      Tile<kWenoTileRows[0]>::NTHREAD, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, weno_stage_mixed_batch_kernel<1>,
-                                                      Tile<kWenoTileRows[1]>::NTHREAD, 0);
-    return n;
+    switch (variant) {
+        case 0: return occupancy_v<0>();
+        case 1: return occupancy_v<1>();
+        case 2: return occupancy_v<2>();
+        case 3: return occupancy_v<3>();
+        case 4: return occupancy_v<4>();
+        case 5: return occupancy_v<5>();
+        default: return 0;
+    }
 }
 
 cudaError_t launch_weno_stage_mixed(const CUtensorMap& tmap, const double* Ucur, const double* Un, double* Uout,
