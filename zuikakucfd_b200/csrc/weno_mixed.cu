@@ -19,6 +19,7 @@
 // down to a 16-byte boundary) into shared memory; the completion wait is
 // bounded and reports STATUS_TIMEOUT instead of hanging.
 #include "batch.cuh"
+#include "f32x2.cuh"
 #include "tma.cuh"
 #include "tma_host.h"
 #include "zk_common.cuh"
@@ -67,13 +68,7 @@ __device__ __forceinline__ void weno5(T UL2, T UL1, T UP, T UR1, T UR2, T UR3, T
     UR = (e0 * qR0 + e1 * qR1 + e2 * qR2) / (e0 + e1 + e2);
 }
 
-// Packed FP32 pairs (sm_100 add/mul/fma .f32x2): one instruction issues the
-// same operation for two conserved variables.  Each lane rounds exactly as the
-// scalar instruction does; reciprocals stay per lane (MUFU has no pair form).
-__device__ __forceinline__ float2 f2(float s) { return make_float2(s, s); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// Reciprocals of packed pairs stay per lane (MUFU has no pair form).
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
