@@ -221,6 +221,7 @@ typedef struct zk_batch_options {
     size_t arena_bytes;   /* > 0: one device allocation all problems carve from    */
     int weno_variant;     /* -1: tuned; 0..5: pin the WENO tile variant (the      */
                           /* autotuner then tunes CTAs per SM only)               */
+    int dg_variant;       /* -1: tuned; 0..3: pin the mixed DG tile variant       */
 } zk_batch_options;
 
 typedef struct zk_batch_report {
@@ -258,9 +259,10 @@ int zk_batch_problem_info(zk_batch* b, int id, zk_batch_problem* out);
 int zk_batch_dt_history(zk_batch* b, int id, double* dts, int n);
 /* Chosen configuration of group g (groups form at zk_batch_run): tile variant
  * of the stage kernel (WENO: 3 * h + k, tile height {4, 8}[h] worked by
- * {rows/2 + 1, rows + 1, 2 rows + 2}[k] warps; mixed DG: index into the tile
- * heights {2, 4}) and its CTAs per SM; *ngroups = number of groups.  Any
- * pointer may be NULL; g = -1 only reports the number of groups. */
+ * {rows/2 + 1, rows + 1, 2 rows + 2}[k] warps; mixed DG: 2 * t + h, tile
+ * height {2, 4}[h] at t + 1 threads per cell) and its CTAs per SM; *ngroups =
+ * number of groups.  Any pointer may be NULL; g = -1 only reports the number
+ * of groups. */
 int zk_batch_group_config(zk_batch* b, int g, int* method, int* precision, int* order, int* variant,
                           int* ctas_per_sm, int* ngroups);
 /* Tile of group g's stage kernel: cells per tile (tile_rows x tile_cols) and

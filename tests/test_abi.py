@@ -62,9 +62,11 @@ def test_batch_default_options_and_bad_options(lib):
     lib.zk_last_error.restype = C.c_char_p
     o = zk_batch_options()
     lib.zk_batch_default_options(C.byref(o))
-    assert (o.device, o.policy, o.graph_steps, o.autotune, o.arena_bytes, o.weno_variant) == (0, 0, 10, 1, 0, -1)
+    assert (o.device, o.policy, o.graph_steps, o.autotune, o.arena_bytes) == (0, 0, 10, 1, 0)
+    assert (o.weno_variant, o.dg_variant) == (-1, -1)
     h = C.c_void_p()
-    for field, bad, word in (("weno_variant", 6, b"weno_variant"), ("graph_steps", 0, b"graph_steps"),
+    for field, bad, word in (("weno_variant", 6, b"weno_variant"), ("dg_variant", 4, b"dg_variant"),
+                             ("graph_steps", 0, b"graph_steps"),
                              ("autotune", 3, b"autotune"), ("policy", 9, b"policy")):
         lib.zk_batch_default_options(C.byref(o))
         setattr(o, field, bad)

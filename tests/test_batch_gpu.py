@@ -104,7 +104,7 @@ def test_batch_matches_single_problems(policy, active, gsteps):
                 assert r in (4, 8) and g["tile_cols"] == 32
                 assert g["threads_per_tile"] // 32 in (r // 2 + 1, r + 1, 2 * r + 2)
             elif g["precision"] == "mixed":
-                assert g["tile_rows"] in (2, 4) and g["threads_per_cell"] == 1.0
+                assert g["tile_rows"] in (2, 4) and g["threads_per_cell"] in (1.0, 2.0)
 
 
 @pytest.mark.parametrize("variant", range(6))
@@ -124,6 +124,30 @@ def test_batch_weno_tile_variants(variant):
         for g in bt.groups():
             assert g["variant"] == variant and g["tile_rows"] == rows
             assert g["threads_per_tile"] == 32 * (rows // 2 + 1, rows + 1, 2 * rows + 2)[variant % 3]
+
+
+@pytest.mark.parametrize("variant", range(4))
+def test_batch_dg_tile_variants(variant):
+    """Every mixed DG tile variant (tile height x one or two threads per
+    cell, pinned instead of tuned) gives the single-run states bit for bit,
+    with the reference limiter, HLLC and periodic boundaries."""
+    from zuikakucfd_b200.batch import Batch
+    from zuikakucfd_b200 import cases
+    specs = [s for s in _specs() if s["method"] == "dg" and s["precision"] == "mixed"]
+    c = cases.four_quadrant(45, seed=18, ny=34)
+    specs.append(dict(bctype=c.bctype, da=c.da, gamma=c.gamma, state=c.dg_state(1), nsteps=6, cfl=0.5,
+                      method="dg", order=1, precision="mixed"))
+    with Batch(policy="all", graph_steps=4, autotune=1, dg_variant=variant) as bt:
+        ids = [bt.add(**s) for s in specs]
+        rep = bt.run()
+        assert rep["done"] == len(specs)
+        for pid, spec in zip(ids, specs):
+            ref, lams = _single(spec, bt.dt_history(pid))
+            assert [_cfl_dt(spec, lam) for lam in lams] == list(bt.dt_history(pid))
+            assert np.array_equal(bt.get_state(pid), ref), (variant, spec["order"])
+        for g in bt.groups():
+            assert g["variant"] == variant and g["tile_rows"] == (2, 4)[variant & 1]
+            assert g["threads_per_cell"] == 1.0 + (variant >> 1)
 
 
 def test_batch_failure_stays_local():

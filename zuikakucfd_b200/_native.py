@@ -41,7 +41,7 @@ class zk_options(C.Structure):
 class zk_batch_options(C.Structure):
     _fields_ = [("device", C.c_int), ("policy", C.c_int), ("active_cells", C.c_double),
                 ("graph_steps", C.c_int), ("autotune", C.c_int), ("arena_bytes", C.c_size_t),
-                ("weno_variant", C.c_int)]
+                ("weno_variant", C.c_int), ("dg_variant", C.c_int)]
 
 
 class zk_batch_report(C.Structure):

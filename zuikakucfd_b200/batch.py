@@ -24,7 +24,8 @@ from . import cases
 
 class Batch:
     def __init__(self, policy: str = "all", active_cells: float = 8e6, graph_steps: int = 10,
-                 autotune: int = 1, arena_bytes: int = 0, device: int = 0, weno_variant: int = -1):
+                 autotune: int = 1, arena_bytes: int = 0, device: int = 0, weno_variant: int = -1,
+                 dg_variant: int = -1):
         L = N.lib()
         o = N.zk_batch_options()
         L.zk_batch_default_options(C.byref(o))
@@ -35,6 +36,7 @@ class Batch:
         o.autotune = int(autotune)
         o.arena_bytes = int(arena_bytes)
         o.weno_variant = int(weno_variant)
+        o.dg_variant = int(dg_variant)
         h = C.c_void_p()
         N.check(L.zk_batch_create(C.byref(o), C.byref(h)))
         self._h = h

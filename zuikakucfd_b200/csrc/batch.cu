@@ -244,12 +244,12 @@ double stage_flops(const zk_options& o) {
 
 // Time the tile variants x persistent grid sizes of group g's stage-1 kernel
 // on a sample of its problems (up to 8M updated cells); keep the fastest.  A
-// pinned WENO variant is timed alone and its result is not cached.
+// pinned variant is timed alone and its result is not cached.
 int autotune(zk_batch* b, BGroup& g) {
     int dev = 0;
     BK_CUDA(cudaGetDevice(&dev));
     const auto key = std::make_tuple(dev, g.method, g.precision, g.order);
-    const bool pinned = !g.dg() && b->opt.weno_variant >= 0;
+    const bool pinned = g.dg() ? (g.mixed() && b->opt.dg_variant >= 0) : b->opt.weno_variant >= 0;
     if (b->opt.autotune == 1 && !pinned) {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune.find(key);
@@ -270,7 +270,7 @@ int autotune(zk_batch* b, BGroup& g) {
     for (int s : sample) adm[g.members[s]] = 1;
     BK_CUDA(cudaMemcpyAsync(b->d_admitted, adm.data(), sizeof(int) * adm.size(), cudaMemcpyHostToDevice, b->stream));
     const bool fp64dg = g.dg() && !g.mixed();
-    const int nvar = (fp64dg || pinned) ? 1 : g.dg() ? 2 : kWenoVariants;
+    const int nvar = (fp64dg || pinned) ? 1 : g.dg() ? kDgVariants : kWenoVariants;
     float best = 3.0e38f;
     int best_v = g.variant, best_c = g.ctas;
     for (int v = 0; v < nvar; ++v) {
@@ -469,7 +469,8 @@ int finalize(zk_batch* b) {
                                     b->stream));
             BK_CUDA(cudaStreamSynchronize(b->stream));
         }
-        g.variant = g.dg() ? 1 : b->opt.weno_variant >= 0 ? b->opt.weno_variant : kWenoDefaultVariant;
+        if (!g.dg()) g.variant = b->opt.weno_variant >= 0 ? b->opt.weno_variant : kWenoDefaultVariant;
+        else g.variant = (g.mixed() && b->opt.dg_variant >= 0) ? b->opt.dg_variant : kDgDefaultVariant;
         g.ctas = occupancy(g, g.variant);
         if (g.dg() && !g.mixed()) g.ctas_cell = dg_fp64_batch_occupancy(g.order, 1);
         if (g.ctas <= 0) return bfail(ZK_ERR_CUDA, "stage kernel of group %d cannot be resident", (int)gi);
@@ -496,6 +497,7 @@ void zk_batch_default_options(zk_batch_options* o) {
     o->autotune = 1;
     o->arena_bytes = 0;
     o->weno_variant = -1;
+    o->dg_variant = -1;
 }
 
 int zk_batch_create(const zk_batch_options* o, zk_batch** out) {
@@ -506,6 +508,8 @@ int zk_batch_create(const zk_batch_options* o, zk_batch** out) {
     if (o->autotune < 0 || o->autotune > 2) return bfail(ZK_ERR_ARG, "autotune must be 0, 1 or 2");
     if (o->weno_variant < -1 || o->weno_variant >= kWenoVariants)
         return bfail(ZK_ERR_ARG, "weno_variant must be -1 or 0..%d", kWenoVariants - 1);
+    if (o->dg_variant < -1 || o->dg_variant >= kDgVariants)
+        return bfail(ZK_ERR_ARG, "dg_variant must be -1 or 0..%d", kDgVariants - 1);
     BK_CUDA(cudaSetDevice(o->device));
     zk_batch* b = new zk_batch();
     b->opt = *o;
@@ -794,8 +798,8 @@ int zk_batch_group_tile(zk_batch* b, int g, int* tile_rows, int* tile_cols, int*
         rows = weno_variant_rows(G.variant);
         threads = 32 * weno_variant_warps(G.variant);
     } else if (G.mixed()) {
-        rows = kDgTileRows[G.variant];
-        threads = rows * cols;
+        rows = dg_variant_rows(G.variant);
+        threads = rows * cols * dg_variant_tpc(G.variant);
     } else {
         cols = kDgCellBlock;  // the FP64 DG cell pass
         threads = cols;

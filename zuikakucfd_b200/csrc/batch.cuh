@@ -51,8 +51,14 @@ constexpr int weno_tile_warps(int rows, int k) { return k == 0 ? rows / 2 + 1 : 
 constexpr int weno_variant_rows(int v) { return kWenoTileRows[v / 3]; }
 constexpr int weno_variant_warps(int v) { return weno_tile_warps(kWenoTileRows[v / 3], v % 3); }
 constexpr int kWenoDefaultVariant = 4;  // 32 x 8, 9 warps
-// Tile heights of the mixed-precision DG stage kernel (one thread per cell).
+// Tile variants of the mixed-precision DG stage kernel: v = 2 * t + h is a
+// 32 x kDgTileRows[h] tile worked by t + 1 threads per cell (two threads
+// split a cell's four conserved variables into pairs).
 constexpr int kDgTileRows[2] = {2, 4};
+constexpr int kDgVariants = 4;
+constexpr int dg_variant_rows(int v) { return kDgTileRows[v & 1]; }
+constexpr int dg_variant_tpc(int v) { return 1 + (v >> 1); }
+constexpr int kDgDefaultVariant = 1;  // 32 x 4, one thread per cell
 // Row segment of the FP64 DG cell pass (one thread per cell).
 constexpr int kDgCellBlock = 64;
 

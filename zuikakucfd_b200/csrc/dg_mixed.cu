@@ -152,6 +152,46 @@ __device__ __forceinline__ void hlle_dg_f(const float L[4], const float R[4], fl
     }
 }
 
+// Combine and limiter arithmetic of the mixed stage, shared by the one- and
+// two-thread-per-cell kernels.  Every operation is rounded explicitly (no
+// contraction left to the compiler), so both kernels produce the same bits.
+// Shu-Osher stages 2 and 3 in FP64: 3/4 un + 1/4 w, 1/3 un + 2/3 w (one
+// fused multiply-add each).
+__device__ __forceinline__ double so_combine(int stage, double un, double w) {
+    return stage == 2 ? __fma_rn(0.75, un, __dmul_rn(0.25, w)) : __fma_rn(1.0 / 3.0, un, __dmul_rn(2.0 / 3.0, w));
+}
+// |m|^2 / 2 rho
+__device__ __forceinline__ float half_m2_over_rho(float rho, float mx, float my) {
+    return __fdividef(__fmul_rn(0.5f, __fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my))), rho);
+}
+// (gamma - 1)(E - |m|^2 / 2 rho)
+__device__ __forceinline__ float pressure_f(float g1, float rho, float mx, float my, float E) {
+    return __fmul_rn(g1, __fsub_rn(E, half_m2_over_rho(rho, mx, my)));
+}
+// Zhang-Shu ratio (avg - lo) / (avg - x + eps)
+__device__ __forceinline__ float zs_ratio(float avg, float lo, float x, float eps) {
+    return __fdividef(__fsub_rn(avg, lo), __fadd_rn(__fsub_rn(avg, x), eps));
+}
+// Persson indicator of one variable's modes (src_DG/fluid.cpp:824-870): the
+// factor for its highest modes, 1 when the variable is not limited.
+template <int P, int NM>
+__device__ __forceinline__ float persson_factor(const float (&d)[NM], float s0) {
+    constexpr int NQ = P + 1;
+    float Et = 0.0f, Ep = 0.0f;
+#pragma unroll
+    for (int m = 0; m < NM; ++m) {
+        const float x = __fmul_rn(d[m], d[m]);
+        Et = __fadd_rn(Et, x);
+        if (m / NQ == P || m % NQ == P) Ep = __fadd_rn(Ep, x);
+    }
+    const float s = __log10f(__fdividef(Ep, __fadd_rn(Et, 1e-5f)));
+    if (!(s > s0)) return 1.0f;
+    const float eps = (s > s0 + 1.0f)
+                          ? 1.0f
+                          : __fmul_rn(0.5f, __fadd_rn(1.0f, __sinf(__fmul_rn(3.14159265f, __fsub_rn(__fsub_rn(s, s0), 0.5f)))));
+    return __fsub_rn(1.0f, eps);
+}
+
 // Floats per cell slot in shared memory: 4*NM rounded so that (stride/4) is
 // odd, which puts 8 consecutive cells' 16-byte loads in 8 distinct bank groups.
 __host__ __device__ constexpr int vpitch(int nm) { return ((4 * nm / 4) % 2 == 1) ? 4 * nm : 4 * nm + 4; }
@@ -475,14 +515,14 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         for (int e = 0; e < 4; ++e) {
             const int v = v4 + e, q = v / NM, m = v % NM;
             const double un = a.un[(size_t)v * plane + k];
-            const double dd = dt * (double)acc[q][m];
+            const double du = (double)acc[q][m];
             double o;
             if (a.stage == 1) {
-                o = un + dd;
+                o = __fma_rn(dt, du, un);
             } else {
-                const double w = (double)cv[e] + dd;
+                const double w = __fma_rn(dt, du, (double)cv[e]);
                 cv[e] = (float)w;
-                o = (a.stage == 2) ? 0.75 * un + 0.25 * w : (1.0 / 3.0) * un + (2.0 / 3.0) * w;
+                o = so_combine(a.stage, un, w);
             }
             acc[q][m] = (float)o;
         }
@@ -498,28 +538,19 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         if (kd == KIND_UPDATED) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                float Et = 0.0f, Ep = 0.0f;
-#pragma unroll
-                for (int m = 0; m < NM; ++m) {
-                    const float x = acc[q][m] * acc[q][m];
-                    Et += x;
-                    if (m / NQ == P || m % NQ == P) Ep += x;
-                }
-                const float s = log10f(Ep / (Et + 1e-5f));
-                if (s > a.s0) {
-                    const float eps = (s > a.s0 + 1.0f) ? 1.0f : 0.5f * (1.0f + sinf(3.14159265f * ((s - a.s0) - 0.5f)));
-                    pf[q] = 1.0f - eps;
+                pf[q] = persson_factor<P, NM>(acc[q], a.s0);
+                if (pf[q] != 1.0f) {
 #pragma unroll
                     for (int m = 0; m < NM; ++m)
-                        if (m / NQ == P || m % NQ == P) acc[q][m] *= pf[q];
+                        if (m / NQ == P || m % NQ == P) acc[q][m] = __fmul_rn(acc[q][m], pf[q]);
                 }
             }
         }
         const float RHO_MIN = 1e-5f, P_MIN = 1e-5f, EPS = 1e-5f, g1 = a.gamma - 1.0f;
         if (acc[0][0] < RHO_MIN) { acc[0][0] = RHO_MIN; rho_clamp = true; }
         const float rho0 = acc[0][0], mx0 = acc[1][0], my0 = acc[2][0];
-        const float ke0 = 0.5f * (mx0 * mx0 + my0 * my0) / rho0;
-        if (g1 * (acc[3][0] - ke0) < P_MIN) { acc[3][0] = P_MIN / g1 + ke0; e_fix = true; }
+        const float ke0 = half_m2_over_rho(rho0, mx0, my0);
+        if (__fmul_rn(g1, __fsub_rn(acc[3][0], ke0)) < P_MIN) { acc[3][0] = __fadd_rn(__fdividef(P_MIN, g1), ke0); e_fix = true; }
         // Zhang-Shu points (4 x 4 Gauss grid, cubic factors zero): separable
         // evaluation, first over px at node a, then over py at node b
         constexpr int NZ = NQ < 3 ? NQ : 3;
@@ -539,16 +570,16 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
                 float rho = 0.0f;
 #pragma unroll
                 for (int py = 0; py < NZ; ++py) rho = fmaf(t[py], S.Z[py][zb], rho);
-                if (rho < RHO_MIN) th = fminr(th, (rho0 - RHO_MIN) / (rho0 - rho + EPS));
+                if (rho < RHO_MIN) th = fminr(th, zs_ratio(rho0, RHO_MIN, rho, EPS));
             }
         }
         if (th < 1.0f) {
 #pragma unroll
             for (int m = 1; m < NM; ++m)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q][m] *= th;
+                for (int q = 0; q < 4; ++q) acc[q][m] = __fmul_rn(acc[q][m], th);
         }
-        const float p_avg = g1 * (acc[3][0] - 0.5f * (acc[1][0] * acc[1][0] + acc[2][0] * acc[2][0]) / acc[0][0]);
+        const float p_avg = pressure_f(g1, acc[0][0], acc[1][0], acc[2][0], acc[3][0]);
         float tp = 1.0f;
 #pragma unroll 1
         for (int za = 0; za < 4; ++za) {
@@ -573,15 +604,15 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
                     U[q] = x;
                 }
                 if (U[0] <= RHO_MIN) continue;
-                const float p = g1 * (U[3] - 0.5f * (U[1] * U[1] + U[2] * U[2]) / U[0]);
-                if (p < P_MIN) tp = fminr(tp, (p_avg - P_MIN) / (p_avg - p + EPS));
+                const float p = pressure_f(g1, U[0], U[1], U[2], U[3]);
+                if (p < P_MIN) tp = fminr(tp, zs_ratio(p_avg, P_MIN, p, EPS));
             }
         }
         if (tp < 1.0f) {
 #pragma unroll
             for (int m = 1; m < NM; ++m)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) acc[q][m] *= tp;
+                for (int q = 0; q < 4; ++q) acc[q][m] = __fmul_rn(acc[q][m], tp);
         }
         theta = th * tp;
     }
@@ -600,10 +631,11 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
         double e0 = 0.0;
         if (e_fix) {
-            const double rho0 = rho_clamp ? 1e-5 : (1.0 / 3.0) * a.un[k] + (2.0 / 3.0) * (double)sd[slot * VP];
-            const double mx0 = (1.0 / 3.0) * a.un[(size_t)NM * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + NM];
-            const double my0 = (1.0 / 3.0) * a.un[(size_t)2 * NM * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + 2 * NM];
-            e0 = 1e-5 / (double)(a.gamma - 1.0f) + 0.5 * (mx0 * mx0 + my0 * my0) / rho0;
+            const double rho0 = rho_clamp ? 1e-5 : so_combine(3, a.un[k], (double)sd[slot * VP]);
+            const double mx0 = so_combine(3, a.un[(size_t)NM * plane + k], (double)sd[slot * VP + NM]);
+            const double my0 = so_combine(3, a.un[(size_t)2 * NM * plane + k], (double)sd[slot * VP + 2 * NM]);
+            e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
+                           __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
         }
         double cs[4][4] = {};  // LAM: variable q at corner e
 #pragma unroll
@@ -611,13 +643,13 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
 #pragma unroll
             for (int m = 0; m < NM; ++m) {
                 const int v = q * NM + m;
-                double o = (1.0 / 3.0) * a.un[(size_t)v * plane + k] + (2.0 / 3.0) * (double)sd[slot * VP + v];
+                double o = so_combine(3, a.un[(size_t)v * plane + k], (double)sd[slot * VP + v]);
                 if (m == 0) {
                     if (q == 0 && rho_clamp) o = 1e-5;
                     if (q == 3 && e_fix) o = e0;
                 } else {
-                    if (m / NQ == P || m % NQ == P) o *= (double)pf[q];
-                    o *= (double)theta;
+                    if (m / NQ == P || m % NQ == P) o = __dmul_rn(o, (double)pf[q]);
+                    o = __dmul_rn(o, (double)theta);
                 }
                 out[(size_t)v * plane + k] = (TOut)o;
                 if (LAM)
@@ -628,6 +660,538 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         if (kd == KIND_UPDATED) {
             const double rho = out[k], mx = out[(size_t)NM * plane + k], my = out[(size_t)2 * NM * plane + k];
             const double p = (double)(a.gamma - 1.0f) * (out[(size_t)3 * NM * plane + k] - 0.5 * (mx * mx + my * my) / rho);
+            if (!(p > 0.0)) flags |= STATUS_P;
+        }
+    }
+    if (flags) atomicOr(a.status, flags);
+    return umax;
+}
+
+// Own half (two variables, 2 NM floats, contiguous in a cell-major slot) as
+// vectors of VW floats.
+template <int NM>
+struct HalfVec {
+    static constexpr int VW = (2 * NM) % 4 == 0 ? 4 : 2;
+};
+template <int VW>
+__device__ __forceinline__ void load_vec(const float* p, float (&x)[VW]) {
+    if constexpr (VW == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+    } else {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        x[0] = v.x; x[1] = v.y;
+    }
+}
+template <int VW>
+__device__ __forceinline__ void store_vec(float* p, const float (&x)[VW]) {
+    if constexpr (VW == 4) *reinterpret_cast<float4*>(p) = make_float4(x[0], x[1], x[2], x[3]);
+    else *reinterpret_cast<float2*>(p) = make_float2(x[0], x[1]);
+}
+
+// The four variables from this half's pair (a0, a1) and the partner's
+// (o0, o1): half 0 owns variables 0, 1, half 1 owns 2, 3.
+__device__ __forceinline__ void join_pair(int h, float a0, float a1, float o0, float o1, float (&U)[4]) {
+    U[0] = h ? o0 : a0;
+    U[1] = h ? o1 : a1;
+    U[2] = h ? a0 : o0;
+    U[3] = h ? a1 : o1;
+}
+
+// stage_tile with two threads per cell: lanes 2i and 2i + 1 share cell i of
+// the tile and half h = lane & 1 owns variables 2h, 2h + 1 (traces,
+// transforms, accumulators, Persson factor, combine, output).  What needs all
+// four variables at a point -- the fluxes at every quadrature point and face
+// point, the Zhang-Shu pressure, the positivity check -- swaps the pair with
+// the partner lane and is evaluated by both halves.  Every value is formed
+// with the operations, in the order, of stage_tile, so the two give the same
+// bits.  Shuffles run under masks taken by ballot over lanes that are all
+// present: the face loop has a warp-uniform trip count and the cell phase
+// returns only after its last shuffle.
+template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
+__device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int i0, float* smem) {
+    constexpr int MNT = MTX * MTY, NT = 2 * MNT, SY = MTY + 2;
+    constexpr int NQ = P + 1, NM = NQ * NQ;
+    constexpr int SD = SX * SY;
+    constexpr int VP = vpitch(NM);
+    constexpr int VW = HalfVec<NM>::VW;
+    constexpr unsigned FULL = 0xffffffffu;
+    const DGSepF& S = c_sepf[P - 1];
+    float* sd = smem;
+    float* sfx = sd + VP * SD;
+    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);
+
+    const int tid = threadIdx.x, h = tid & 1, ci = tid >> 1;
+    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
+    const size_t plane = a.g.plane;
+
+    // U^n of this half's variables, towards L2 (read again only by the combine)
+    {
+        const int pr = ci / MTX, pc = ci - pr * MTX;
+        if (i0 + pr < ny && j0 + pc < nx) {
+            const double* u0 = a.un + (size_t)(2 * h * NM) * plane + (size_t)(i0 + pr) * pitch + (j0 + pc);
+#pragma unroll 8
+            for (int v = 0; v < 2 * NM; ++v)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(u0 + (size_t)v * plane));
+        }
+    }
+
+    // 0. gather tile + halo (as stage_tile, over all NT threads)
+    for (int slot = tid; slot < SD; slot += NT) {
+        const int r = slot / SX, c = slot - r * SX;
+        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        uint8_t kd = KIND_PASSIVE;
+        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+            const size_t k = (size_t)gi * pitch + gj;
+            kd = a.kind[k] & KIND_MASK;
+            size_t ks = k;
+            int neg = -1;
+            if (kd >= KIND_COPY) {
+                ks = (size_t)a.gsrc[k];
+                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
+            }
+            if (sizeof(TIn) == 4) {
+                const float* src = static_cast<const float*>(a.cur) + ks;
+#pragma unroll 8
+                for (int v = 0; v < 4 * NM; ++v) {
+                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
+                                 : "memory");
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                if (neg >= 0)
+                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
+            } else {
+#pragma unroll 4
+                for (int v = 0; v < 4 * NM; v += 4) {
+                    float4 x;
+                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
+                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
+                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
+                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
+                    if (neg == (v + 0) / NM) x.x = -x.x;
+                    if (neg == (v + 1) / NM) x.y = -x.y;
+                    if (neg == (v + 2) / NM) x.z = -x.z;
+                    if (neg == (v + 3) / NM) x.w = -x.w;
+                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
+                }
+            }
+        } else {
+            for (int v = 0; v < 4 * NM; v += 4)
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        sk[slot] = kd;
+    }
+    __syncthreads();
+
+    // 1. interface fluxes, one face per lane pair; the trip count is the same
+    //    for every lane (idle pairs take the last face and store nothing)
+    constexpr int NXF = MTY * (MTX + 1), NYF = (MTY + 1) * MTX, NF = NXF + NYF;
+    for (int base = 0; base < NF; base += MNT) {
+        const int f0 = base + ci;
+        const int f = f0 < NF ? f0 : NF - 1;
+        int sl, sr;
+        float* dst;
+        int dstride;
+        bool ydir;
+        if (f < NXF) {
+            const int r = f / (MTX + 1), c = f - r * (MTX + 1);
+            sl = (r + 1) * SX + c;
+            sr = sl + 1;
+            dst = sfx + r * (MTX + 1) + c;
+            dstride = MTY * (MTX + 1);
+            ydir = false;
+        } else {
+            const int g = f - NXF, r = g / MTX, c = g - r * MTX;
+            sl = r * SX + c + 1;
+            sr = sl + SX;
+            dst = sfy + r * MTX + c;
+            dstride = (MTY + 1) * MTX;
+            ydir = true;
+        }
+        const bool store = f0 < NF && (sk[sl] == KIND_UPDATED || sk[sr] == KIND_UPDATED);
+        float el[2][NQ], er[2][NQ];
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) el[cc][n] = er[cc][n] = 0.0f;
+        const float* pl = sd + sl * VP + 2 * h * NM;
+        const float* pr = sd + sr * VP + 2 * h * NM;
+        if (ydir) {
+#pragma unroll
+            for (int v = 0; v < 2 * NM; v += VW) {
+                float lv[VW], rv[VW];
+                load_vec<VW>(pl + v, lv);
+                load_vec<VW>(pr + v, rv);
+#pragma unroll
+                for (int e = 0; e < VW; ++e) {
+                    const int cc = (v + e) / NM, m = (v + e) % NM, px = m / NQ, py = m % NQ;
+                    el[cc][px] += lv[e];
+                    er[cc][px] += (py & 1) ? -rv[e] : rv[e];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int v = 0; v < 2 * NM; v += VW) {
+                float lv[VW], rv[VW];
+                load_vec<VW>(pl + v, lv);
+                load_vec<VW>(pr + v, rv);
+#pragma unroll
+                for (int e = 0; e < VW; ++e) {
+                    const int cc = (v + e) / NM, m = (v + e) % NM, px = m / NQ, py = m % NQ;
+                    el[cc][py] += lv[e];
+                    er[cc][py] += (px & 1) ? -rv[e] : rv[e];
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            float ul[2], ur[2];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                float x = 0.0f, y = 0.0f;
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) {
+                    x = fmaf(el[cc][n], S.L[n][q], x);
+                    y = fmaf(er[cc][n], S.L[n][q], y);
+                }
+                ul[cc] = x;
+                ur[cc] = y;
+            }
+            float UL[4], UR[4];
+            join_pair(h, ul[0], ul[1], __shfl_xor_sync(FULL, ul[0], 1), __shfl_xor_sync(FULL, ul[1], 1), UL);
+            join_pair(h, ur[0], ur[1], __shfl_xor_sync(FULL, ur[0], 1), __shfl_xor_sync(FULL, ur[1], 1), UR);
+            float Fq[4];
+            if (ydir) {
+                float l[4] = {UL[0], UL[2], UL[1], UL[3]};
+                float r[4] = {UR[0], UR[2], UR[1], UR[3]};
+                float g[4];
+                if (a.hll) hlle_dg_f(l, r, a.gamma, g);
+                else hllc_dg_f(l, r, a.gamma, g);
+                Fq[0] = g[0]; Fq[1] = g[2]; Fq[2] = g[1]; Fq[3] = g[3];
+            } else {
+                if (a.hll) hlle_dg_f(UL, UR, a.gamma, Fq);
+                else hllc_dg_f(UL, UR, a.gamma, Fq);
+            }
+            if (store) {
+                dst[(q * 4 + 2 * h) * dstride] = h ? Fq[2] : Fq[0];
+                dst[(q * 4 + 2 * h + 1) * dstride] = h ? Fq[3] : Fq[1];
+            }
+        }
+    }
+    __syncthreads();
+
+    // 2. one lane pair per cell
+    const int r = ci / MTX, c = ci - r * MTX;
+    const int gi = i0 + r, gj = j0 + c;
+    const bool inside = gi < ny && gj < nx;
+    const unsigned pm = __ballot_sync(FULL, inside);  // lanes of cells in the grid (whole pairs)
+    if (!inside) return 0.0;
+    const int slot = (r + 1) * SX + c + 1;
+    const size_t k = (size_t)gi * pitch + gj;
+    const uint8_t kd = sk[slot];
+    const unsigned um = __ballot_sync(pm, kd == KIND_UPDATED);
+    float acc[2][NM];
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[cc][m] = 0.0f;
+    if (kd == KIND_UPDATED) {
+        const float* pc = sd + slot * VP + 2 * h * NM;
+#pragma unroll 1
+        for (int qa = 0; qa < NQ; ++qa) {
+            float e[2][NQ];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) e[cc][n] = 0.0f;
+#pragma unroll
+            for (int v = 0; v < 2 * NM; v += VW) {
+                float dv[VW];
+                load_vec<VW>(pc + v, dv);
+#pragma unroll
+                for (int u = 0; u < VW; ++u) {
+                    const int cc = (v + u) / NM, m = (v + u) % NM;
+                    e[cc][m % NQ] = fmaf(dv[u], S.L[m / NQ][qa], e[cc][m % NQ]);
+                }
+            }
+            float f[2][NQ], g[2][NQ];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) f[cc][n] = g[cc][n] = 0.0f;
+#pragma unroll
+            for (int qb = 0; qb < NQ; ++qb) {
+                float uo[2];
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) x = fmaf(e[cc][n], S.L[n][qb], x);
+                    uo[cc] = x;
+                }
+                float U[4];
+                join_pair(h, uo[0], uo[1], __shfl_xor_sync(um, uo[0], 1), __shfl_xor_sync(um, uo[1], 1), U);
+                float F[4], G[4];
+                euler_flux_f(U, a.gamma, F, G);
+                const float w = S.W[qa] * S.W[qb];
+                const float Fo[2] = {h ? F[2] : F[0], h ? F[3] : F[1]};
+                const float Go[2] = {h ? G[2] : G[0], h ? G[3] : G[1]};
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    const float Fw = Fo[cc] * w, Gw = Go[cc] * w;
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) {
+                        f[cc][n] = fmaf(Fw, S.L[n][qb], f[cc][n]);
+                        g[cc][n] = fmaf(Gw, S.D[n][qb], g[cc][n]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int px = 0; px < NQ; ++px) {
+                const float dx = S.D[px][qa], lx = S.L[px][qa];
+#pragma unroll
+                for (int py = 0; py < NQ; ++py)
+#pragma unroll
+                    for (int cc = 0; cc < 2; ++cc)
+                        acc[cc][px * NQ + py] = fmaf(dx, f[cc][py], fmaf(lx, g[cc][py], acc[cc][px * NQ + py]));
+            }
+        }
+        // face integrals of this half's variables (order of stage_tile)
+        {
+            const float* Fr = sfx + r * (MTX + 1) + c + 1;
+            const float* Fl = sfx + r * (MTX + 1) + c;
+            const float* Fd = sfy + (r + 1) * MTX + c;
+            const float* Fu = sfy + r * MTX + c;
+            constexpr int fsx = MTY * (MTX + 1), fsy = (MTY + 1) * MTX;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const int u = 2 * h + cc;
+                float hr[NQ], hl[NQ], hd[NQ], hu[NQ];
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) hr[n] = hl[n] = hd[n] = hu[n] = 0.0f;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    const float xr = Fr[(q * 4 + u) * fsx], xl = Fl[(q * 4 + u) * fsx];
+                    const float xd = Fd[(q * 4 + u) * fsy], xu = Fu[(q * 4 + u) * fsy];
+#pragma unroll
+                    for (int n = 0; n < NQ; ++n) {
+                        const float wl = S.WL[n][q];
+                        hr[n] = fmaf(wl, xr, hr[n]);
+                        hl[n] = fmaf(wl, xl, hl[n]);
+                        hd[n] = fmaf(wl, xd, hd[n]);
+                        hu[n] = fmaf(wl, xu, hu[n]);
+                    }
+                }
+#pragma unroll
+                for (int px = 0; px < NQ; ++px)
+#pragma unroll
+                    for (int py = 0; py < NQ; ++py) {
+                        float t = acc[cc][px * NQ + py] - hr[py] - hd[px];
+                        t += (px & 1) ? -hl[py] : hl[py];
+                        t += (py & 1) ? -hu[px] : hu[px];
+                        acc[cc][px * NQ + py] = t;
+                    }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < NM; ++m) {
+            const float scale = (float)((2 * (m / NQ) + 1) * (2 * (m % NQ) + 1)) * a.inv2h;
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) acc[cc][m] *= scale;
+        }
+    }
+
+    if (a.stage == 0) {
+#pragma unroll
+        for (int v = 0; v < 2 * NM; ++v)
+            static_cast<TOut*>(a.out)[(size_t)(2 * h * NM + v) * plane + k] = (TOut)acc[v / NM][v % NM];
+        return 0.0;
+    }
+    // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
+    const double dt = a.dt;
+    float* pw = sd + slot * VP + 2 * h * NM;
+#pragma unroll
+    for (int v = 0; v < 2 * NM; v += VW) {
+        float cv[VW];
+        load_vec<VW>(pw + v, cv);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) {
+            const int vv = v + e, cc = vv / NM, m = vv % NM;
+            const double un = a.un[(size_t)(2 * h * NM + vv) * plane + k];
+            const double du = (double)acc[cc][m];
+            double o;
+            if (a.stage == 1) {
+                o = __fma_rn(dt, du, un);
+            } else {
+                const double w = __fma_rn(dt, du, (double)cv[e]);
+                cv[e] = (float)w;
+                o = so_combine(a.stage, un, w);
+            }
+            acc[cc][m] = (float)o;
+        }
+        if (a.stage != 1) store_vec<VW>(pw + v, cv);  // own slot, own half
+    }
+    __syncwarp(pm);  // the partner's half of the slot (w) is read below
+
+    // limiter decisions in FP32 (src_DG/fluid.cpp:824-992), as factors
+    float pf[2] = {1.0f, 1.0f};
+    float theta = 1.0f;
+    bool rho_clamp = false, e_fix = false;
+    const bool in_range = gi >= 3 && gi < ny - 3 && gj >= 3 && gj < nx - 3;
+    const bool lim = a.limiter == ZK_LIMITER_REFERENCE && in_range;
+    const unsigned lm = __ballot_sync(pm, lim);
+    if (lim) {
+        if (kd == KIND_UPDATED) {
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                pf[cc] = persson_factor<P, NM>(acc[cc], a.s0);
+                if (pf[cc] != 1.0f) {
+#pragma unroll
+                    for (int m = 0; m < NM; ++m)
+                        if (m / NQ == P || m % NQ == P) acc[cc][m] = __fmul_rn(acc[cc][m], pf[cc]);
+                }
+            }
+        }
+        const float RHO_MIN = 1e-5f, P_MIN = 1e-5f, EPS = 1e-5f, g1 = a.gamma - 1.0f;
+        float m0[4];  // the cell means of all four variables
+        join_pair(h, acc[0][0], acc[1][0], __shfl_xor_sync(lm, acc[0][0], 1), __shfl_xor_sync(lm, acc[1][0], 1), m0);
+        if (m0[0] < RHO_MIN) { m0[0] = RHO_MIN; rho_clamp = true; }
+        const float rho0 = m0[0], mx0 = m0[1], my0 = m0[2];
+        const float ke0 = half_m2_over_rho(rho0, mx0, my0);
+        if (__fmul_rn(g1, __fsub_rn(m0[3], ke0)) < P_MIN) { m0[3] = __fadd_rn(__fdividef(P_MIN, g1), ke0); e_fix = true; }
+        acc[0][0] = h ? m0[2] : m0[0];
+        acc[1][0] = h ? m0[3] : m0[1];
+        // Zhang-Shu points (4 x 4 Gauss grid, cubic factors zero), separable;
+        // the density pass runs on half 0's variable 0 and is shared
+        constexpr int NZ = NQ < 3 ? NQ : 3;
+        float th = 1.0f;
+#pragma unroll 1
+        for (int za = 0; za < 4; ++za) {
+            float t[NZ];
+#pragma unroll
+            for (int py = 0; py < NZ; ++py) {
+                float x = 0.0f;
+#pragma unroll
+                for (int px = 0; px < NZ; ++px) x = fmaf(acc[0][px * NQ + py], S.Z[px][za], x);
+                t[py] = x;
+            }
+#pragma unroll
+            for (int zb = 0; zb < 4; ++zb) {
+                float rho = 0.0f;
+#pragma unroll
+                for (int py = 0; py < NZ; ++py) rho = fmaf(t[py], S.Z[py][zb], rho);
+                if (rho < RHO_MIN) th = fminr(th, zs_ratio(rho0, RHO_MIN, rho, EPS));
+            }
+        }
+        {
+            const float tho = __shfl_xor_sync(lm, th, 1);
+            th = h ? tho : th;
+        }
+        if (th < 1.0f) {
+#pragma unroll
+            for (int m = 1; m < NM; ++m)
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) acc[cc][m] = __fmul_rn(acc[cc][m], th);
+        }
+        const float p_avg = pressure_f(g1, m0[0], m0[1], m0[2], m0[3]);
+        float tp = 1.0f;
+#pragma unroll 1
+        for (int za = 0; za < 4; ++za) {
+            float t[2][NZ];
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+                for (int py = 0; py < NZ; ++py) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int px = 0; px < NZ; ++px) x = fmaf(acc[cc][px * NQ + py], S.Z[px][za], x);
+                    t[cc][py] = x;
+                }
+#pragma unroll
+            for (int zb = 0; zb < 4; ++zb) {
+                float uo[2];
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) {
+                    float x = 0.0f;
+#pragma unroll
+                    for (int py = 0; py < NZ; ++py) x = fmaf(t[cc][py], S.Z[py][zb], x);
+                    uo[cc] = x;
+                }
+                float U[4];
+                join_pair(h, uo[0], uo[1], __shfl_xor_sync(lm, uo[0], 1), __shfl_xor_sync(lm, uo[1], 1), U);
+                if (U[0] <= RHO_MIN) continue;
+                const float p = pressure_f(g1, U[0], U[1], U[2], U[3]);
+                if (p < P_MIN) tp = fminr(tp, zs_ratio(p_avg, P_MIN, p, EPS));
+            }
+        }
+        if (tp < 1.0f) {
+#pragma unroll
+            for (int m = 1; m < NM; ++m)
+#pragma unroll
+                for (int cc = 0; cc < 2; ++cc) acc[cc][m] = __fmul_rn(acc[cc][m], tp);
+        }
+        theta = th * tp;
+    }
+
+    uint32_t flags = 0;
+    double umax = 0.0;
+    if (kd == KIND_UPDATED) {
+        if (!isfinite(h ? acc[1][0] : acc[0][0])) flags |= STATUS_NAN;  // rho (half 0) or E (half 1)
+        if (h == 0 && !(acc[0][0] > 0.0f)) flags |= STATUS_RHO;
+    }
+    TOut* out = static_cast<TOut*>(a.out);
+    if (sizeof(TOut) == 4) {
+#pragma unroll
+        for (int v = 0; v < 2 * NM; ++v) out[(size_t)(2 * h * NM + v) * plane + k] = (TOut)acc[v / NM][v % NM];
+    } else {
+        // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
+        double e0 = 0.0;
+        if (e_fix && h == 1) {
+            const double rho0 = rho_clamp ? 1e-5 : so_combine(3, a.un[k], (double)sd[slot * VP]);
+            const double mx0 = so_combine(3, a.un[(size_t)NM * plane + k], (double)sd[slot * VP + NM]);
+            const double my0 = so_combine(3, a.un[(size_t)2 * NM * plane + k], (double)sd[slot * VP + 2 * NM]);
+            e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
+                           __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
+        }
+        double cs[4][2] = {};  // LAM: this half's variables at corner e
+        double om[2] = {0.0, 0.0};  // this half's written cell means
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const int q = 2 * h + cc, v = q * NM + m;
+                double o = so_combine(3, a.un[(size_t)v * plane + k], (double)sd[slot * VP + v]);
+                if (m == 0) {
+                    if (q == 0 && rho_clamp) o = 1e-5;
+                    if (q == 3 && e_fix) o = e0;
+                    om[cc] = o;
+                } else {
+                    if (m / NQ == P || m % NQ == P) o = __dmul_rn(o, (double)pf[cc]);
+                    o = __dmul_rn(o, (double)theta);
+                }
+                out[(size_t)v * plane + k] = (TOut)o;
+                if (LAM)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) cs[e][cc] = __dadd_rn(cs[e][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+            }
+        if (LAM) {
+            double full[4][4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const double o0 = __shfl_xor_sync(pm, cs[e][0], 1), o1 = __shfl_xor_sync(pm, cs[e][1], 1);
+                full[e][0] = h ? o0 : cs[e][0];
+                full[e][1] = h ? o1 : cs[e][1];
+                full[e][2] = h ? cs[e][0] : o0;
+                full[e][3] = h ? cs[e][1] : o1;
+            }
+            if (a.kind[k] & KIND_FLUID) umax = dg_cell_speed(full, a.gamma64, 0.0);
+        }
+        const double p0 = __shfl_xor_sync(pm, om[0], 1), p1 = __shfl_xor_sync(pm, om[1], 1);
+        if (kd == KIND_UPDATED && h == 0) {
+            const double rho = om[0], mx = om[1], my = p0, E = p1;
+            const double p = (double)(a.gamma - 1.0f) * (E - 0.5 * (mx * mx + my * my) / rho);
             if (!(p > 0.0)) flags |= STATUS_P;
         }
     }
@@ -649,14 +1213,42 @@ __global__ void __launch_bounds__(MTX * 4, P == 1 ? 8 : 3) dg_stage_mixed_kernel
     stage_tile<P, TIn, TOut, 4>(a, blockIdx.x * MTX, blockIdx.y * 4, smem);
 }
 
+// The same stage with two threads per cell (stage_tile_pair).  Register
+// shares: 1024 threads per SM for P = 1, 768 for P = 2 (80 registers, no
+// spills), 512 for P = 3 (2 CTAs of 8 warps at 128 registers; 768 spilled 300
+// bytes and ran 17% slower).
+constexpr int pair_thread_budget(int P) { return P == 1 ? 1024 : P == 3 ? 512 : 768; }
+template <int P>
+constexpr int pair_min_blocks() {
+    return batch_min_blocks(MTX * 8, pair_thread_budget(P), smem_bytes<P, 4>());
+}
+template <int P, typename TIn, typename TOut>
+__global__ void __launch_bounds__(MTX * 8, pair_min_blocks<P>()) dg_stage_mixed_pair_kernel(MixArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    stage_tile_pair<P, TIn, TOut, 4>(a, blockIdx.x * MTX, blockIdx.y * 4, smem);
+}
+
+// Threads per cell of the single-problem stage kernel, per P (measured at
+// 2048^2, four-quadrant, GDOF/s): P = 1 34.2 (one) vs 26.5 (two), P = 2 37.2
+// vs 33.4, P = 3 29.7-30.3 vs 31.1.
+constexpr int kSingleTpc[4] = {0, 1, 1, 2};
+
 // Persistent stage STAGE over every listed problem of a batch group, tile
-// variant V (kDgTileRows[V] rows): stage 1 reads U^n (FP64) and writes F[0],
-// stage 2 reads F[0] and writes F[1], stage 3 reads F[1] and writes U^n and
-// leaves the new state's max wave speed in the problem's control block.
+// variant V (dg_variant_rows(V) rows, dg_variant_tpc(V) threads per cell):
+// stage 1 reads U^n (FP64) and writes F[0], stage 2 reads F[0] and writes
+// F[1], stage 3 reads F[1] and writes U^n and leaves the new state's max wave
+// speed in the problem's control block.  Register shares: one thread per
+// cell, 1024 (P = 1) or 384 threads per SM; two, pair_thread_budget(P).
+template <int P, int V>
+constexpr int batch_blocks() {
+    constexpr int MTY = dg_variant_rows(V);
+    return dg_variant_tpc(V) == 1 ? (P == 1 ? 32 : 12) / MTY
+                                  : batch_min_blocks(MTX * MTY * 2, pair_thread_budget(P), smem_bytes<P, MTY>());
+}
 template <int P, int STAGE, int V>
-__global__ void __launch_bounds__(MTX * kDgTileRows[V], (P == 1 ? 32 : 12) / kDgTileRows[V])
+__global__ void __launch_bounds__(MTX * dg_variant_rows(V) * dg_variant_tpc(V), batch_blocks<P, V>())
     dg_stage_mixed_batch_kernel(const DgItem* __restrict__ items, const int* __restrict__ dir, int cap) {
-    constexpr int MTY = kDgTileRows[V];
+    constexpr int MTY = dg_variant_rows(V);
     using TIn = typename std::conditional<STAGE == 1, double, float>::type;
     using TOut = typename std::conditional<STAGE == 3, double, float>::type;
     extern __shared__ __align__(16) float smem[];
@@ -684,7 +1276,9 @@ __global__ void __launch_bounds__(MTX * kDgTileRows[V], (P == 1 ? 32 : 12) / kDg
         }
         __syncthreads();
         if (s_org[2]) {
-            const double m = stage_tile<P, TIn, TOut, MTY, STAGE == 3>(sa, s_org[0], s_org[1], smem);
+            double m;
+            if constexpr (dg_variant_tpc(V) == 1) m = stage_tile<P, TIn, TOut, MTY, STAGE == 3>(sa, s_org[0], s_org[1], smem);
+            else m = stage_tile_pair<P, TIn, TOut, MTY, STAGE == 3>(sa, s_org[0], s_org[1], smem);
             if (STAGE == 3) block_max_commit_to(m, s_lam);  // the next step's wave speed
         }
         __syncthreads();
@@ -693,8 +1287,8 @@ __global__ void __launch_bounds__(MTX * kDgTileRows[V], (P == 1 ? 32 : 12) / kDg
 
 template <int P, int STAGE, int V>
 cudaError_t batch_one(const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s, int* occ) {
-    constexpr size_t sm = smem_bytes<P, kDgTileRows[V]>();
-    constexpr int nt = MTX * kDgTileRows[V];
+    constexpr size_t sm = smem_bytes<P, dg_variant_rows(V)>();
+    constexpr int nt = MTX * dg_variant_rows(V) * dg_variant_tpc(V);
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -722,24 +1316,31 @@ cudaError_t batch_pv(int stage, const DgItem* items, const int* dir, int cap, in
 template <int P>
 cudaError_t batch_p(int variant, int stage, const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s,
                     int* occ) {
-    return variant == 0 ? batch_pv<P, 0>(stage, items, dir, cap, grid, s, occ)
-                        : batch_pv<P, 1>(stage, items, dir, cap, grid, s, occ);
+    static_assert(kDgVariants == 4, "one case per tile variant");
+    switch (variant) {
+        case 0: return batch_pv<P, 0>(stage, items, dir, cap, grid, s, occ);
+        case 1: return batch_pv<P, 1>(stage, items, dir, cap, grid, s, occ);
+        case 2: return batch_pv<P, 2>(stage, items, dir, cap, grid, s, occ);
+        case 3: return batch_pv<P, 3>(stage, items, dir, cap, grid, s, occ);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 template <int P, typename TIn, typename TOut>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
     constexpr size_t sm = smem_bytes<P, 4>();
+    constexpr bool pair = kSingleTpc[P] == 2;
+    auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut> : dg_stage_mixed_kernel<P, TIn, TOut>;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(dg_stage_mixed_kernel<P, TIn, TOut>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
     dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + 3) / 4);
-    dg_stage_mixed_kernel<P, TIn, TOut><<<grid, MTX * 4, sm, s>>>(a);
+    kern<<<grid, MTX * 4 * kSingleTpc[P], sm, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -815,7 +1416,7 @@ int dg_mixed_batch_occupancy(int P, int variant, int stage) {
 
 // Tiles of one problem for tile variant v.
 int dg_mixed_batch_tiles(int variant, int ny, int nx) {
-    return ((nx + MTX - 1) / MTX) * ((ny + kDgTileRows[variant] - 1) / kDgTileRows[variant]);
+    return ((nx + MTX - 1) / MTX) * ((ny + dg_variant_rows(variant) - 1) / dg_variant_rows(variant));
 }
 
 // One mixed-precision DG stage: cur (double if in_fp64 else float) -> out
