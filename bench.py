@@ -369,8 +369,9 @@ def main():
             if w["method"] == "weno":
                 kname = "weno_stage_fp64_kernel" if prec == "fp64" else "weno_stage_mixed_kernel"
             else:
+                # the mixed P=3 stage runs two threads per cell (dg_mixed.cu kSingleTpc)
                 kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if prec == "fp64"
-                         else "dg_stage_mixed_kernel")
+                         else "dg_stage_mixed_pair_kernel" if w["order"] == 3 else "dg_stage_mixed_kernel")
             roofs[prec] = {
                 "bound": "fp64" if prec == "fp64" else "fp32", "achieved": achieved, "peak": pk,
                 "unit": "TFLOP/s", "frac": achieved / pk, "traffic": None,
