@@ -504,29 +504,32 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         for (int v = 0; v < 4 * NM; ++v) static_cast<TOut*>(a.out)[(size_t)v * plane + k] = (TOut)acc[v / NM][v % NM];
         return 0.0;
     }
-    // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
+    // combine in FP64 (w = cur + dt dU at stages 2, 3); an FP64 output is
+    // written here, and the limiter later rewrites only the modes it changes
     const double dt = a.dt;
-    float* pw = sd + slot * VP;
+    const float* pw = sd + slot * VP;
+    TOut* out = static_cast<TOut*>(a.out);
+    constexpr bool OUT64 = sizeof(TOut) == 8;
+    double cs[4][4] = {};  // LAM: variable q at corner e of the written state
 #pragma unroll
     for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
-        float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
-        float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+        const float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
+        const float cv[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int v = v4 + e, q = v / NM, m = v % NM;
             const double un = a.un[(size_t)v * plane + k];
             const double du = (double)acc[q][m];
-            double o;
-            if (a.stage == 1) {
-                o = __fma_rn(dt, du, un);
-            } else {
-                const double w = __fma_rn(dt, du, (double)cv[e]);
-                cv[e] = (float)w;
-                o = so_combine(a.stage, un, w);
-            }
+            const double o = a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
             acc[q][m] = (float)o;
+            if (OUT64) {
+                out[(size_t)v * plane + k] = (TOut)o;
+                if (LAM)
+#pragma unroll
+                    for (int cn = 0; cn < 4; ++cn)
+                        cs[cn][q] = __dadd_rn(cs[cn][q], __dmul_rn(o, __ldg(a.phic + m * 4 + cn)));
+            }
         }
-        if (a.stage != 1) *reinterpret_cast<float4*>(pw + v4) = make_float4(cv[0], cv[1], cv[2], cv[3]);  // own slot
     }
 
     // limiter decisions in FP32 (src_DG/fluid.cpp:824-992), as factors
@@ -623,39 +626,46 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         if (!isfinite(acc[0][0]) || !isfinite(acc[3][0])) flags |= STATUS_NAN;
         if (!(acc[0][0] > 0.0f)) flags |= STATUS_RHO;
     }
-    TOut* out = static_cast<TOut*>(a.out);
-    if (sizeof(TOut) == 4) {
+    if (!OUT64) {
 #pragma unroll
         for (int v = 0; v < 4 * NM; ++v) out[(size_t)v * plane + k] = (TOut)acc[v / NM][v % NM];
     } else {
-        // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
-        double e0 = 0.0;
-        if (e_fix) {
-            const double rho0 = rho_clamp ? 1e-5 : so_combine(3, a.un[k], (double)sd[slot * VP]);
-            const double mx0 = so_combine(3, a.un[(size_t)NM * plane + k], (double)sd[slot * VP + NM]);
-            const double my0 = so_combine(3, a.un[(size_t)2 * NM * plane + k], (double)sd[slot * VP + 2 * NM]);
-            e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
-                           __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
-        }
-        double cs[4][4] = {};  // LAM: variable q at corner e
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                const int v = q * NM + m;
-                double o = so_combine(3, a.un[(size_t)v * plane + k], (double)sd[slot * VP + v]);
-                if (m == 0) {
-                    if (q == 0 && rho_clamp) o = 1e-5;
-                    if (q == 3 && e_fix) o = e0;
-                } else {
-                    if (m / NQ == P || m % NQ == P) o = __dmul_rn(o, (double)pf[q]);
-                    o = __dmul_rn(o, (double)theta);
-                }
-                out[(size_t)v * plane + k] = (TOut)o;
-                if (LAM)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) cs[e][q] = __dadd_rn(cs[e][q], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+        // U^(n+1) in FP64 is in place: apply the limiter's factors to the modes
+        // they change, on the values the combine wrote
+        if (rho_clamp || e_fix || theta != 1.0f || pf[0] != 1.0f || pf[1] != 1.0f || pf[2] != 1.0f ||
+            pf[3] != 1.0f) {
+            double e0 = 0.0;
+            if (e_fix) {
+                const double rho0 = rho_clamp ? 1e-5 : (double)out[k];
+                const double mx0 = out[(size_t)NM * plane + k], my0 = out[(size_t)2 * NM * plane + k];
+                e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
+                               __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
             }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) cs[e][q] = 0.0;
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const size_t idx = (size_t)(q * NM + m) * plane + k;
+                    double o = out[idx];
+                    if (m == 0) {
+                        if (q == 0 && rho_clamp) out[idx] = o = 1e-5;
+                        if (q == 3 && e_fix) out[idx] = o = e0;
+                    } else {
+                        const bool border = m / NQ == P || m % NQ == P;
+                        if ((border && pf[q] != 1.0f) || theta != 1.0f) {
+                            if (border) o = __dmul_rn(o, (double)pf[q]);
+                            o = __dmul_rn(o, (double)theta);
+                            out[idx] = o;
+                        }
+                    }
+                    if (LAM)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) cs[e][q] = __dadd_rn(cs[e][q], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+                }
+            }
+        }
         if (LAM && (a.kind[k] & KIND_FLUID)) umax = dg_cell_speed(cs, a.gamma64, 0.0);
         if (kd == KIND_UPDATED) {
             const double rho = out[k], mx = out[(size_t)NM * plane + k], my = out[(size_t)2 * NM * plane + k];
@@ -1009,9 +1019,14 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             static_cast<TOut*>(a.out)[(size_t)(2 * h * NM + v) * plane + k] = (TOut)acc[v / NM][v % NM];
         return 0.0;
     }
-    // combine in FP64; keep w = cur + dt*dU (stage >= 2) for the FP64 rewrite
+    // combine in FP64 (w = cur + dt dU at stages 2, 3); an FP64 output is
+    // written here, and the limiter later rewrites only the modes it changes
     const double dt = a.dt;
-    float* pw = sd + slot * VP + 2 * h * NM;
+    const float* pw = sd + slot * VP + 2 * h * NM;
+    TOut* out = static_cast<TOut*>(a.out);
+    constexpr bool OUT64 = sizeof(TOut) == 8;
+    double cs[4][2] = {};       // LAM: this half's variables at corner e of the written state
+    double om[2] = {0.0, 0.0};  // this half's written cell means
 #pragma unroll
     for (int v = 0; v < 2 * NM; v += VW) {
         float cv[VW];
@@ -1021,19 +1036,19 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             const int vv = v + e, cc = vv / NM, m = vv % NM;
             const double un = a.un[(size_t)(2 * h * NM + vv) * plane + k];
             const double du = (double)acc[cc][m];
-            double o;
-            if (a.stage == 1) {
-                o = __fma_rn(dt, du, un);
-            } else {
-                const double w = __fma_rn(dt, du, (double)cv[e]);
-                cv[e] = (float)w;
-                o = so_combine(a.stage, un, w);
-            }
+            const double o = a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
             acc[cc][m] = (float)o;
+            if (OUT64) {
+                out[(size_t)(2 * h * NM + vv) * plane + k] = (TOut)o;
+                if (m == 0) om[cc] = o;
+                if (LAM)
+#pragma unroll
+                    for (int cn = 0; cn < 4; ++cn)
+                        cs[cn][cc] = __dadd_rn(cs[cn][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + cn)));
+            }
         }
-        if (a.stage != 1) store_vec<VW>(pw + v, cv);  // own slot, own half
     }
-    __syncwarp(pm);  // the partner's half of the slot (w) is read below
+    __syncwarp(pm);  // the partner's written cell means are read below
 
     // limiter decisions in FP32 (src_DG/fluid.cpp:824-992), as factors
     float pf[2] = {1.0f, 1.0f};
@@ -1141,41 +1156,47 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         if (!isfinite(h ? acc[1][0] : acc[0][0])) flags |= STATUS_NAN;  // rho (half 0) or E (half 1)
         if (h == 0 && !(acc[0][0] > 0.0f)) flags |= STATUS_RHO;
     }
-    TOut* out = static_cast<TOut*>(a.out);
-    if (sizeof(TOut) == 4) {
+    if (!OUT64) {
 #pragma unroll
         for (int v = 0; v < 2 * NM; ++v) out[(size_t)(2 * h * NM + v) * plane + k] = (TOut)acc[v / NM][v % NM];
     } else {
-        // U^(n+1) in FP64: (1/3) U^n + (2/3) w, with the limiter's factors
-        double e0 = 0.0;
-        if (e_fix && h == 1) {
-            const double rho0 = rho_clamp ? 1e-5 : so_combine(3, a.un[k], (double)sd[slot * VP]);
-            const double mx0 = so_combine(3, a.un[(size_t)NM * plane + k], (double)sd[slot * VP + NM]);
-            const double my0 = so_combine(3, a.un[(size_t)2 * NM * plane + k], (double)sd[slot * VP + 2 * NM]);
-            e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
-                           __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
-        }
-        double cs[4][2] = {};  // LAM: this half's variables at corner e
-        double om[2] = {0.0, 0.0};  // this half's written cell means
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-            for (int m = 0; m < NM; ++m) {
-                const int q = 2 * h + cc, v = q * NM + m;
-                double o = so_combine(3, a.un[(size_t)v * plane + k], (double)sd[slot * VP + v]);
-                if (m == 0) {
-                    if (q == 0 && rho_clamp) o = 1e-5;
-                    if (q == 3 && e_fix) o = e0;
-                    om[cc] = o;
-                } else {
-                    if (m / NQ == P || m % NQ == P) o = __dmul_rn(o, (double)pf[cc]);
-                    o = __dmul_rn(o, (double)theta);
-                }
-                out[(size_t)v * plane + k] = (TOut)o;
-                if (LAM)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) cs[e][cc] = __dadd_rn(cs[e][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+        // U^(n+1) in FP64 is in place: apply the limiter's factors to the modes
+        // of this half they change, on the values the combine wrote
+        if (rho_clamp || e_fix || theta != 1.0f || pf[0] != 1.0f || pf[1] != 1.0f) {
+            double e0 = 0.0;
+            if (e_fix && h == 1) {  // rho and m_x means: the partner's, written before the syncwarp
+                const double rho0 = rho_clamp ? 1e-5 : (double)out[k];
+                const double mx0 = out[(size_t)NM * plane + k], my0 = om[0];
+                e0 = __dadd_rn(__ddiv_rn(1e-5, (double)(a.gamma - 1.0f)),
+                               __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
             }
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) cs[e][cc] = 0.0;
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const int q = 2 * h + cc;
+                    const size_t idx = (size_t)(q * NM + m) * plane + k;
+                    double o = out[idx];
+                    if (m == 0) {
+                        if (q == 0 && rho_clamp) out[idx] = o = 1e-5;
+                        if (q == 3 && e_fix) out[idx] = o = e0;
+                        om[cc] = o;
+                    } else {
+                        const bool border = m / NQ == P || m % NQ == P;
+                        if ((border && pf[cc] != 1.0f) || theta != 1.0f) {
+                            if (border) o = __dmul_rn(o, (double)pf[cc]);
+                            o = __dmul_rn(o, (double)theta);
+                            out[idx] = o;
+                        }
+                    }
+                    if (LAM)
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) cs[e][cc] = __dadd_rn(cs[e][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+                }
+            }
+        }
         if (LAM) {
             double full[4][4];
 #pragma unroll

@@ -259,8 +259,11 @@ constexpr int kTvbRows = 1;  // rows per CTA
 template <typename T, int P>
 __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gated, int i, int j);
 
+// 6 CTAs per SM (80 registers, some spilled): the pass is latency-bound, and
+// the extra resident warps beat the 4 CTAs that 110 registers allowed (+1.9%
+// on the gated P=3 mixed step; 8 CTAs at 64 registers slowed the FP64 pass).
 template <typename T, int P>
-__global__ void __launch_bounds__(128) tvb_kernel(TvbArgs a) {
+__global__ void __launch_bounds__(128, 6) tvb_kernel(TvbArgs a) {
     __shared__ __align__(16) MlpSmem S;
     const bool gated = a.mlp != nullptr;  // uniform over the grid
     if (gated) {
