@@ -153,8 +153,9 @@ __device__ __forceinline__ void hlle_dg_f(const float L[4], const float R[4], fl
 }
 
 // Combine and limiter arithmetic of the mixed stage, shared by the one- and
-// two-thread-per-cell kernels.  Every operation is rounded explicitly (no
-// contraction left to the compiler), so both kernels produce the same bits.
+// two-thread-per-cell kernels.  Every operation is rounded explicitly (fused
+// multiply-adds written as such, nothing left to the compiler's contraction),
+// so both kernels produce the same bits.
 // Shu-Osher stages 2 and 3 in FP64: 3/4 un + 1/4 w, 1/3 un + 2/3 w (one
 // fused multiply-add each).
 __device__ __forceinline__ double so_combine(int stage, double un, double w) {
@@ -162,7 +163,7 @@ __device__ __forceinline__ double so_combine(int stage, double un, double w) {
 }
 // |m|^2 / 2 rho
 __device__ __forceinline__ float half_m2_over_rho(float rho, float mx, float my) {
-    return __fdividef(__fmul_rn(0.5f, __fadd_rn(__fmul_rn(mx, mx), __fmul_rn(my, my))), rho);
+    return __fdividef(__fmul_rn(0.5f, __fmaf_rn(mx, mx, __fmul_rn(my, my))), rho);
 }
 // (gamma - 1)(E - |m|^2 / 2 rho)
 __device__ __forceinline__ float pressure_f(float g1, float rho, float mx, float my, float E) {
@@ -180,9 +181,8 @@ __device__ __forceinline__ float persson_factor(const float (&d)[NM], float s0) 
     float Et = 0.0f, Ep = 0.0f;
 #pragma unroll
     for (int m = 0; m < NM; ++m) {
-        const float x = __fmul_rn(d[m], d[m]);
-        Et = __fadd_rn(Et, x);
-        if (m / NQ == P || m % NQ == P) Ep = __fadd_rn(Ep, x);
+        Et = __fmaf_rn(d[m], d[m], Et);
+        if (m / NQ == P || m % NQ == P) Ep = __fmaf_rn(d[m], d[m], Ep);
     }
     const float s = __log10f(__fdividef(Ep, __fadd_rn(Et, 1e-5f)));
     if (!(s > s0)) return 1.0f;
@@ -510,7 +510,6 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     const float* pw = sd + slot * VP;
     TOut* out = static_cast<TOut*>(a.out);
     constexpr bool OUT64 = sizeof(TOut) == 8;
-    double cs[4][4] = {};  // LAM: variable q at corner e of the written state
 #pragma unroll
     for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
         const float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
@@ -522,13 +521,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
             const double du = (double)acc[q][m];
             const double o = a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
             acc[q][m] = (float)o;
-            if (OUT64) {
-                out[(size_t)v * plane + k] = (TOut)o;
-                if (LAM)
-#pragma unroll
-                    for (int cn = 0; cn < 4; ++cn)
-                        cs[cn][q] = __dadd_rn(cs[cn][q], __dmul_rn(o, __ldg(a.phic + m * 4 + cn)));
-            }
+            if (OUT64) out[(size_t)v * plane + k] = (TOut)o;
         }
     }
 
@@ -642,31 +635,41 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
                                __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) cs[e][q] = 0.0;
+            for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int m = 0; m < NM; ++m) {
                     const size_t idx = (size_t)(q * NM + m) * plane + k;
-                    double o = out[idx];
                     if (m == 0) {
-                        if (q == 0 && rho_clamp) out[idx] = o = 1e-5;
-                        if (q == 3 && e_fix) out[idx] = o = e0;
+                        if (q == 0 && rho_clamp) out[idx] = 1e-5;
+                        if (q == 3 && e_fix) out[idx] = e0;
                     } else {
                         const bool border = m / NQ == P || m % NQ == P;
                         if ((border && pf[q] != 1.0f) || theta != 1.0f) {
+                            double o = out[idx];
                             if (border) o = __dmul_rn(o, (double)pf[q]);
-                            o = __dmul_rn(o, (double)theta);
-                            out[idx] = o;
+                            out[idx] = __dmul_rn(o, (double)theta);
                         }
                     }
-                    if (LAM)
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) cs[e][q] = __dadd_rn(cs[e][q], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
                 }
-            }
         }
-        if (LAM && (a.kind[k] & KIND_FLUID)) umax = dg_cell_speed(cs, a.gamma64, 0.0);
+        if (LAM) {
+            // corner values of the state written, accumulated over the modes in
+            // increasing order (read back: nothing extra stays live in registers)
+            double cs[4][4];
+#pragma unroll 1
+            for (int q = 0; q < 4; ++q) {  // one variable at a time: bounded live loads
+                double cq[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const double o = out[(size_t)(q * NM + m) * plane + k];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) cq[e] = __dadd_rn(cq[e], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+                }
+#pragma unroll
+                for (int e = 0; e < 4; ++e) cs[e][q] = cq[e];
+            }
+            if (a.kind[k] & KIND_FLUID) umax = dg_cell_speed(cs, a.gamma64, 0.0);
+        }
         if (kd == KIND_UPDATED) {
             const double rho = out[k], mx = out[(size_t)NM * plane + k], my = out[(size_t)2 * NM * plane + k];
             const double p = (double)(a.gamma - 1.0f) * (out[(size_t)3 * NM * plane + k] - 0.5 * (mx * mx + my * my) / rho);
@@ -1025,7 +1028,6 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     const float* pw = sd + slot * VP + 2 * h * NM;
     TOut* out = static_cast<TOut*>(a.out);
     constexpr bool OUT64 = sizeof(TOut) == 8;
-    double cs[4][2] = {};       // LAM: this half's variables at corner e of the written state
     double om[2] = {0.0, 0.0};  // this half's written cell means
 #pragma unroll
     for (int v = 0; v < 2 * NM; v += VW) {
@@ -1041,10 +1043,6 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             if (OUT64) {
                 out[(size_t)(2 * h * NM + vv) * plane + k] = (TOut)o;
                 if (m == 0) om[cc] = o;
-                if (LAM)
-#pragma unroll
-                    for (int cn = 0; cn < 4; ++cn)
-                        cs[cn][cc] = __dadd_rn(cs[cn][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + cn)));
             }
         }
     }
@@ -1171,33 +1169,35 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                                __ddiv_rn(__dmul_rn(0.5, __dadd_rn(__dmul_rn(mx0, mx0), __dmul_rn(my0, my0))), rho0));
             }
 #pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) cs[e][cc] = 0.0;
+            for (int cc = 0; cc < 2; ++cc)
 #pragma unroll
                 for (int m = 0; m < NM; ++m) {
                     const int q = 2 * h + cc;
                     const size_t idx = (size_t)(q * NM + m) * plane + k;
-                    double o = out[idx];
                     if (m == 0) {
-                        if (q == 0 && rho_clamp) out[idx] = o = 1e-5;
-                        if (q == 3 && e_fix) out[idx] = o = e0;
-                        om[cc] = o;
+                        if (q == 0 && rho_clamp) out[idx] = om[cc] = 1e-5;
+                        if (q == 3 && e_fix) out[idx] = om[cc] = e0;
                     } else {
                         const bool border = m / NQ == P || m % NQ == P;
                         if ((border && pf[cc] != 1.0f) || theta != 1.0f) {
+                            double o = out[idx];
                             if (border) o = __dmul_rn(o, (double)pf[cc]);
-                            o = __dmul_rn(o, (double)theta);
-                            out[idx] = o;
+                            out[idx] = __dmul_rn(o, (double)theta);
                         }
                     }
-                    if (LAM)
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) cs[e][cc] = __dadd_rn(cs[e][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
                 }
-            }
         }
         if (LAM) {
+            // corner values of this half's variables in the state written (read back)
+            double cs[4][2] = {};
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+                for (int m = 0; m < NM; ++m) {
+                    const double o = out[(size_t)((2 * h + cc) * NM + m) * plane + k];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) cs[e][cc] = __dadd_rn(cs[e][cc], __dmul_rn(o, __ldg(a.phic + m * 4 + e)));
+                }
             double full[4][4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
