@@ -192,6 +192,38 @@ __device__ __forceinline__ float persson_factor(const float (&d)[NM], float s0) 
     return __fsub_rn(1.0f, eps);
 }
 
+// Zhang-Shu point values use the modes with px, py < NZ = min(P + 1, 3), and
+// every factor is a Legendre value (|P_n| <= 1 on [-1, 1]), so a variable's
+// point values stay within its mean +- zs_spread.  A pass whose every point
+// provably stays above its floor returns exactly 1 and is skipped.
+template <int P, int NM>
+__device__ __forceinline__ float zs_spread(const float (&d)[NM]) {
+    constexpr int NQ = P + 1, NZ = NQ < 3 ? NQ : 3;
+    float s = 0.0f;
+#pragma unroll
+    for (int px = 0; px < NZ; ++px)
+#pragma unroll
+        for (int py = 0; py < NZ; ++py)
+            if (px || py) s += fabsf(d[px * NQ + py]);
+    return s;
+}
+// every point value of a variable with mean a and spread sp exceeds lo (with a
+// 1e-5 relative margin for the rounding of the bound and of the point values)
+__device__ __forceinline__ bool zs_above(float a, float sp, float lo) {
+    return a - sp - 1e-5f * (fabsf(a) + sp) > lo;
+}
+// every point pressure exceeds p_min: lower bound (gamma-1)(E_lo - |m|_hi^2 /
+// 2 rho_lo) from the four means and spreads, with the same margin
+__device__ __forceinline__ bool zs_p_above(const float (&mean)[4], const float (&sp)[4], float g1, float rho_min,
+                                           float p_min) {
+    const float rlo = mean[0] - sp[0] - 1e-5f * (fabsf(mean[0]) + sp[0]);
+    if (!(rlo > rho_min)) return false;
+    const float mx = fabsf(mean[1]) + sp[1], my = fabsf(mean[2]) + sp[2];
+    const float ke = 0.5f * (mx * mx + my * my) / rlo;
+    const float plo = g1 * (mean[3] - sp[3] - ke) - 1e-5f * g1 * (fabsf(mean[3]) + sp[3] + ke);
+    return plo > p_min;
+}
+
 // Floats per cell slot in shared memory: 4*NM rounded so that (stride/4) is
 // odd, which puts 8 consecutive cells' 16-byte loads in 8 distinct bank groups.
 __host__ __device__ constexpr int vpitch(int nm) { return ((4 * nm / 4) % 2 == 1) ? 4 * nm : 4 * nm + 4; }
@@ -551,8 +583,9 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         // evaluation, first over px at node a, then over py at node b
         constexpr int NZ = NQ < 3 ? NQ : 3;
         float th = 1.0f;
+        const bool rho_pass = !zs_above(rho0, zs_spread<P, NM>(acc[0]), RHO_MIN);
 #pragma unroll 1
-        for (int za = 0; za < 4; ++za) {
+        for (int za = 0; za < (rho_pass ? 4 : 0); ++za) {
             float t[NZ];
 #pragma unroll
             for (int py = 0; py < NZ; ++py) {
@@ -577,8 +610,15 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
         }
         const float p_avg = pressure_f(g1, acc[0][0], acc[1][0], acc[2][0], acc[3][0]);
         float tp = 1.0f;
+        bool p_pass;
+        {
+            const float mean[4] = {acc[0][0], acc[1][0], acc[2][0], acc[3][0]};
+            const float sp[4] = {zs_spread<P, NM>(acc[0]), zs_spread<P, NM>(acc[1]), zs_spread<P, NM>(acc[2]),
+                                 zs_spread<P, NM>(acc[3])};
+            p_pass = !zs_p_above(mean, sp, g1, RHO_MIN, P_MIN);
+        }
 #pragma unroll 1
-        for (int za = 0; za < 4; ++za) {
+        for (int za = 0; za < (p_pass ? 4 : 0); ++za) {
             float t[4][NZ];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
@@ -1080,8 +1120,12 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         // the density pass runs on half 0's variable 0 and is shared
         constexpr int NZ = NQ < 3 ? NQ : 3;
         float th = 1.0f;
+        float spo[2] = {zs_spread<P, NM>(acc[0]), zs_spread<P, NM>(acc[1])};  // this half's spreads
+        float sp[4];
+        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], 1), __shfl_xor_sync(lm, spo[1], 1), sp);
+        const bool rho_pass = !zs_above(rho0, sp[0], RHO_MIN);  // the same decision in both halves
 #pragma unroll 1
-        for (int za = 0; za < 4; ++za) {
+        for (int za = 0; za < (rho_pass ? 4 : 0); ++za) {
             float t[NZ];
 #pragma unroll
             for (int py = 0; py < NZ; ++py) {
@@ -1110,8 +1154,14 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         }
         const float p_avg = pressure_f(g1, m0[0], m0[1], m0[2], m0[3]);
         float tp = 1.0f;
+        // the spreads after the density factor (every lane of lm shuffles)
+        spo[0] = zs_spread<P, NM>(acc[0]);
+        spo[1] = zs_spread<P, NM>(acc[1]);
+        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], 1), __shfl_xor_sync(lm, spo[1], 1), sp);
+        const bool p_pass = !zs_p_above(m0, sp, g1, RHO_MIN, P_MIN);  // the same in both halves
+        const unsigned zm = __ballot_sync(lm, p_pass);                 // lanes that run the pressure pass
 #pragma unroll 1
-        for (int za = 0; za < 4; ++za) {
+        for (int za = 0; za < (p_pass ? 4 : 0); ++za) {
             float t[2][NZ];
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc)
@@ -1133,7 +1183,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                     uo[cc] = x;
                 }
                 float U[4];
-                join_pair(h, uo[0], uo[1], __shfl_xor_sync(lm, uo[0], 1), __shfl_xor_sync(lm, uo[1], 1), U);
+                join_pair(h, uo[0], uo[1], __shfl_xor_sync(zm, uo[0], 1), __shfl_xor_sync(zm, uo[1], 1), U);
                 if (U[0] <= RHO_MIN) continue;
                 const float p = pressure_f(g1, U[0], U[1], U[2], U[3]);
                 if (p < P_MIN) tp = fminr(tp, zs_ratio(p_avg, P_MIN, p, EPS));
