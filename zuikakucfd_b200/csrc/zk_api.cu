@@ -40,6 +40,8 @@ int fail(int code, const char* fmt, ...) {
     } while (0)
 
 void free_device(zk_ctx* c) {
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);  // it captured the buffers freed below
+    c->step_graph = nullptr;
     for (void* p : {(void*)c->Un, (void*)c->S1, (void*)c->S2, (void*)c->kind, (void*)c->gsrc,
                     (void*)c->d_max, (void*)c->d_status, (void*)c->d_phic, (void*)c->d_tmp,
                     (void*)c->F1, (void*)c->F2})
@@ -339,14 +341,70 @@ static int weno_step_fp64(zk_ctx* c, double dt) {
     return ZK_OK;
 }
 
-static int enqueue_steps(zk_ctx* c, double dt, int nsteps) {
-    for (int s = 0; s < nsteps; ++s) {
-        int rc;
-        if (c->opt.method == ZK_METHOD_DG) rc = zk_dg_step(c, dt);
-        else if (c->opt.precision == ZK_PREC_MIXED) rc = zk_weno_mixed_step(c, dt);
-        else rc = weno_step_fp64(c, dt);
-        if (rc) return rc;
+static int step_once(zk_ctx* c, double dt) {
+    if (c->opt.method == ZK_METHOD_DG) return zk_dg_step(c, dt);
+    if (c->opt.precision == ZK_PREC_MIXED) return zk_weno_mixed_step(c, dt);
+    return weno_step_fp64(c, dt);
+}
+
+// Steps per captured graph.  A step's launches are the same every step for a
+// given dt (the stage buffers rotate within the step), so kGraphSteps steps
+// are captured once and replayed; small grids, where a stage kernel lasts a
+// few microseconds, then run without host launch gaps.
+constexpr int kGraphSteps = 16;
+
+// c->step_graph for dt: kept while dt and the buffers (freed with the graph
+// by free_device) stay the same.  Leaves it null when capture is not possible
+// (the stream is already being captured by the caller, or the legacy default
+// stream); the caller then launches eagerly.
+static int ensure_step_graph(zk_ctx* c, double dt) {
+    if (c->step_graph && c->step_graph_dt == dt) return ZK_OK;
+    if (c->step_graph) cudaGraphExecDestroy(c->step_graph);
+    c->step_graph = nullptr;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return ZK_OK;
     }
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return ZK_OK;
+    }
+    int rc = ZK_OK;
+    for (int i = 0; i < kGraphSteps && rc == ZK_OK; ++i) rc = step_once(c, dt);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);  // always ends the capture
+    cudaGraphExec_t x = nullptr;
+    cudaError_t ei = cudaSuccess;
+    if (rc == ZK_OK && e == cudaSuccess && g) ei = cudaGraphInstantiate(&x, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (rc != ZK_OK) return rc;
+    if (e != cudaSuccess) return fail(ZK_ERR_CUDA, "step graph capture: %s", cudaGetErrorString(e));
+    if (ei != cudaSuccess) return fail(ZK_ERR_CUDA, "step graph instantiate: %s", cudaGetErrorString(ei));
+    c->step_graph = x;
+    c->step_graph_dt = dt;
+    return ZK_OK;
+}
+
+// nsteps steps: the first eagerly (any first-use set-up of the kernels runs
+// outside a capture), then whole blocks of kGraphSteps as graph replays, then
+// the rest eagerly.  The same kernels in the same order either way.
+static int enqueue_steps(zk_ctx* c, double dt, int nsteps) {
+    int s = 0;
+    if (nsteps > 0) {
+        if (int rc = step_once(c, dt)) return rc;
+        s = 1;
+    }
+    const int blocks = (nsteps - s) / kGraphSteps;
+    if (blocks > 0) {
+        if (int rc = ensure_step_graph(c, dt)) return rc;
+        if (c->step_graph) {
+            for (int b = 0; b < blocks; ++b) ZK_CUDA(cudaGraphLaunch(c->step_graph, c->stream));
+            s += blocks * kGraphSteps;
+        }
+    }
+    for (; s < nsteps; ++s)
+        if (int rc = step_once(c, dt)) return rc;
     return ZK_OK;
 }
 

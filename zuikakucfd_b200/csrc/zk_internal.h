@@ -40,6 +40,9 @@ struct zk_ctx {
     bool mlp_set = false;
     uint8_t* d_flags = nullptr;   // TVB troubled-cell flags of the last pass, pitched
     uint32_t* d_nflag = nullptr;  // cells the TVB passes limited during the last zk_step
+
+    cudaGraphExec_t step_graph = nullptr;  // kGraphSteps steps at step_graph_dt (zk_step)
+    double step_graph_dt = 0.0;
 };
 
 int zk_internal_fail(int code, const char* msg);
