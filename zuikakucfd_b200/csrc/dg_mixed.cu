@@ -1289,14 +1289,18 @@ __global__ void __launch_bounds__(MTX * 4, P == 1 ? 8 : 3) dg_stage_mixed_kernel
 // spills), 512 for P = 3 (2 CTAs of 8 warps at 128 registers; 768 spilled 300
 // bytes and ran 17% slower).
 constexpr int pair_thread_budget(int P) { return P == 1 ? 1024 : P == 3 ? 512 : 768; }
+// Tile rows of the single-problem two-threads-per-cell kernel: 32 x 2 tiles (4
+// CTAs of 128 threads, the same 16 warps per SM) ran 9% slower at P = 3 (the
+// 1-cell halo is 2.1x the tile's cells instead of 1.6x).
+constexpr int kPairRows = 4;
 template <int P>
 constexpr int pair_min_blocks() {
-    return batch_min_blocks(MTX * 8, pair_thread_budget(P), smem_bytes<P, 4>());
+    return batch_min_blocks(MTX * 2 * kPairRows, pair_thread_budget(P), smem_bytes<P, kPairRows>());
 }
 template <int P, typename TIn, typename TOut>
-__global__ void __launch_bounds__(MTX * 8, pair_min_blocks<P>()) dg_stage_mixed_pair_kernel(MixArgs a) {
+__global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P>()) dg_stage_mixed_pair_kernel(MixArgs a) {
     extern __shared__ __align__(16) float smem[];
-    stage_tile_pair<P, TIn, TOut, 4>(a, blockIdx.x * MTX, blockIdx.y * 4, smem);
+    stage_tile_pair<P, TIn, TOut, kPairRows>(a, blockIdx.x * MTX, blockIdx.y * kPairRows, smem);
 }
 
 // Threads per cell of the single-problem stage kernel, per P (measured at
@@ -1399,8 +1403,9 @@ cudaError_t batch_p(int variant, int stage, const DgItem* items, const int* dir,
 
 template <int P, typename TIn, typename TOut>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
-    constexpr size_t sm = smem_bytes<P, 4>();
     constexpr bool pair = kSingleTpc[P] == 2;
+    constexpr int rows = pair ? kPairRows : 4;
+    constexpr size_t sm = smem_bytes<P, rows>();
     auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut> : dg_stage_mixed_kernel<P, TIn, TOut>;
     static bool attr_set[64] = {};
     int dev = 0;
@@ -1410,8 +1415,8 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
-    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + 3) / 4);
-    kern<<<grid, MTX * 4 * kSingleTpc[P], sm, s>>>(a);
+    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + rows - 1) / rows);
+    kern<<<grid, MTX * rows * kSingleTpc[P], sm, s>>>(a);
     return cudaGetLastError();
 }
 
