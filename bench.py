@@ -337,13 +337,17 @@ def main():
     head = "mixed" if "mixed" in paths else "fp64"
     hp = paths[head]
     # equal-L1 diagnostic: both paths advanced the same steps from the same
-    # state; relative L1 difference of the cell-average density
+    # state; relative L1 and Linf differences of the cell-average density and
+    # pressure (primitives rho, u, v, p recovered in FP64)
     eq = None
     if "mixed" in paths:
-        r64 = paths["fp64"]["solver"].recover_primitives()[0]
-        rmx = paths["mixed"]["solver"].recover_primitives()[0]
-        eq = {"rel_l1_density_mixed_vs_fp64": float(np.abs(rmx - r64).sum() / np.abs(r64).sum()),
-              "steps_compared": args.warmup + args.steps}
+        q64 = paths["fp64"]["solver"].recover_primitives()
+        qmx = paths["mixed"]["solver"].recover_primitives()
+        eq = {"steps_compared": args.warmup + args.steps}
+        for name, f in (("density", 0), ("pressure", 3)):
+            d = np.abs(qmx[f] - q64[f])
+            eq[f"rel_l1_{name}_mixed_vs_fp64"] = float(d.sum() / np.abs(q64[f]).sum())
+            eq[f"rel_linf_{name}_mixed_vs_fp64"] = float(d.max() / np.abs(q64[f]).max())
 
     # end to end through the public API with host buffers: the reference
     # driver's loop (computeMaxSpeed -> dt on the host -> updateMesh), state
