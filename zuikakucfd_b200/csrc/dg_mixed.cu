@@ -3,13 +3,16 @@
 // A CTA owns a 32 x 4 tile of cells.  It gathers the tile plus a 1-cell halo
 // of the stage input into shared memory as FP32 (ghosts through the fill
 // source map, slip walls negated), computes every interface flux of the tile
-// once from the two cells' traces (FP32, in shared memory), then each thread
-// runs its cell's volume quadrature and face integrals in FP32 registers.
-// The Shu-Osher combine is FP64 against the FP64 U^n; the Persson +
-// Zhang-Shu limiter decides in FP32 and is applied as per-mode factors to the
-// FP64 combine.  Stage states U^(1), U^(2) are stored in FP32, U^(n+1) in
-// FP64.  This file is compiled with --use_fast_math (FP32 division, sqrt,
-// log10 and sin use the MUFU approximations).
+// once from the two cells' traces (FP32, in shared memory), then runs each
+// cell's volume quadrature and face integrals in FP32 registers, with one
+// thread per cell (stage_tile) or two, each owning a pair of the conserved
+// variables (stage_tile_pair).  The Shu-Osher combine is FP64 against the
+// FP64 U^n; the Persson + Zhang-Shu limiter decides in FP32 and is applied as
+// per-mode factors.  Stage states U^(1), U^(2) are stored in FP32; U^(n+1) is
+// written in FP64 by the combine, and the limiter rewrites the modes it
+// changes.  This file is compiled with --use_fast_math (FP32 division, sqrt,
+// log10 and sin use the MUFU approximations); the combine and limiter
+// arithmetic is rounded explicitly, so both kernels give the same bits.
 #include <cmath>
 #include <cstring>
 #include <mutex>
