@@ -37,12 +37,13 @@ METRIC = "DOF-updates/s on 1 B200: mixed-prec+learned limiter vs plain FP64 at e
 UNIT = "DOF-updates/s"
 
 # Algorithmic work per updated cell per RK stage (face-deduplicated, 1 flop per
-# add/sub/mul/div/sqrt/min/max; derivation in DESIGN.md).
+# add/sub/mul/div/sqrt/min/max): WENO5 = 2 faces x (8 one-sided
+# reconstructions x 66 + HLLC 117) + flux difference 24 + RK combine 12.
 WENO_FLOPS_PER_CELL_STAGE = 1330.0
 
 
-# Algorithmic flops per updated cell per RK stage (face-deduplicated counts;
-# derivation in DESIGN.md).
+# DG: volume NQ^2 (28 NM + 40) + faces 2 NQ (32 NM + 127) + inverse mass 4 NM
+# + RK combine 16 NM, rounded (NM = (P+1)^2 modes, NQ = P+1 points).
 FLOPS_PER_CELL_STAGE = {("weno", 0): WENO_FLOPS_PER_CELL_STAGE, ("dg", 1): 1700.0, ("dg", 2): 5300.0,
                         ("dg", 3): 13200.0}
 
