@@ -12,6 +12,7 @@
 #include <cuda_bf16.h>
 
 #include "dg_common.cuh"
+#include "f32x2.cuh"
 #include "zk_internal.h"
 #include "zk_mlp.h"
 
@@ -155,6 +156,18 @@ __device__ void stage_mlp_weights(MlpSmem& S, const MlpPacked& W) {
     for (int e = threadIdx.x; e < (int)(sizeof(MlpPacked) / 16); e += blockDim.x) dst[e] = src[e];
 }
 
+// gelu_fast on the two lanes of a pair (packed .f32x2 arithmetic, explicit
+// fused multiply-adds whatever this file's contraction flags; tanh per lane):
+// u = K (x + C x^3), 0.5 x (1 + tanh u).
+__device__ __forceinline__ float2 gelu2(float2 x) {
+    const float2 u = mul2(f2(GELU_K), fma2(mul2(f2(GELU_C), mul2(x, x)), x, x));
+    float t0, t1;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t0) : "f"(u.x));
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t1) : "f"(u.y));
+    const float2 hx = mul2(f2(0.5f), x);
+    return fma2(hx, make_float2(t0, t1), hx);
+}
+
 // Hidden layer: acc[mt][nt][4] = A (from a-fragments) x W^T, + bias, GELU.
 template <int KSTEPS>
 __device__ __forceinline__ void mlp_layer(const uint32_t (&a)[2][KSTEPS][4], const uint16_t* w, int wstride,
@@ -179,13 +192,15 @@ __device__ __forceinline__ void mlp_layer(const uint32_t (&a)[2][KSTEPS][4], con
     }
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
-        const float bl = bias[nt * 8 + 2 * q], bh = bias[nt * 8 + 2 * q + 1];
+        const float2 b = make_float2(bias[nt * 8 + 2 * q], bias[nt * 8 + 2 * q + 1]);  // columns 2q, 2q + 1
 #pragma unroll
         for (int mt = 0; mt < 2; ++mt) {
-            h[mt][nt][0] = gelu_fast(h[mt][nt][0] + bl);
-            h[mt][nt][1] = gelu_fast(h[mt][nt][1] + bh);
-            h[mt][nt][2] = gelu_fast(h[mt][nt][2] + bl);
-            h[mt][nt][3] = gelu_fast(h[mt][nt][3] + bh);
+            const float2 lo = gelu2(add2(make_float2(h[mt][nt][0], h[mt][nt][1]), b));
+            const float2 hi = gelu2(add2(make_float2(h[mt][nt][2], h[mt][nt][3]), b));
+            h[mt][nt][0] = lo.x;
+            h[mt][nt][1] = lo.y;
+            h[mt][nt][2] = hi.x;
+            h[mt][nt][3] = hi.y;
         }
     }
 }
