@@ -236,91 +236,18 @@ __device__ __forceinline__ float load_f(const void* p, size_t i) {
     return (float)static_cast<const T*>(p)[i];
 }
 
-// One tile whose top-left cell is (i0, j0), shared memory at `smem`
-// (smem_bytes<P, MTY>()).  Per-thread returns leave only this function: every
-// barrier of the tile precedes them.  LAM (FP64 output only): returns the max
-// corner wave speed of the thread's cell if it is fluid (computeMaxSpeedDG_omp
-// on the FP64 values written), else 0.
-template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
-__device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
-    constexpr int MNT = MTX * MTY, SY = MTY + 2;
+// Every interface flux of a tile once, from the two cells' traces (FP32, in
+// shared memory): faces dealt to the NTHREAD threads in turn, each thread the
+// whole face (all four variables).  Shared by the one- and two-thread-per-cell
+// stages.
+template <int P, int MTY, int NTHREAD>
+__device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* sd, float* sfx, float* sfy,
+                                                 const uint8_t* sk, int tid) {
     constexpr int NQ = P + 1, NM = NQ * NQ;
-    constexpr int SD = SX * SY;  // cell slots of the tile + halo
-    constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
+    constexpr int VP = vpitch(NM);
     const DGSepF& S = c_sepf[P - 1];
-    float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
-    float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
-    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
-    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
-
-    const int tid = threadIdx.x;
-    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
-    const size_t plane = a.g.plane;
-
-    // U^n of this thread's cell is read again only by the combine: start
-    // bringing it into L2 now so those loads overlap the flux work
-    {
-        const int pr = tid / MTX, pc = tid - pr * MTX;
-        if (i0 + pr < ny && j0 + pc < nx) {
-            const double* u0 = a.un + (size_t)(i0 + pr) * pitch + (j0 + pc);
-#pragma unroll 8
-            for (int v = 0; v < 4 * NM; ++v)
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(u0 + (size_t)v * plane));
-        }
-    }
-
-    // 0. gather tile + halo (corners unused)
-    for (int slot = tid; slot < SD; slot += MNT) {
-        const int r = slot / SX, c = slot - r * SX;
-        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        uint8_t kd = KIND_PASSIVE;
-        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
-            const size_t k = (size_t)gi * pitch + gj;
-            kd = a.kind[k] & KIND_MASK;
-            size_t ks = k;
-            int neg = -1;
-            if (kd >= KIND_COPY) {
-                ks = (size_t)a.gsrc[k];
-                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
-            }
-            if (sizeof(TIn) == 4) {
-                // FP32 input: asynchronous 4-byte copies, all in flight at once
-                const float* src = static_cast<const float*>(a.cur) + ks;
-#pragma unroll 8
-                for (int v = 0; v < 4 * NM; ++v) {
-                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
-                                 : "memory");
-                }
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                if (neg >= 0)
-                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
-            } else {
-#pragma unroll 4
-                for (int v = 0; v < 4 * NM; v += 4) {
-                    float4 x;
-                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
-                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
-                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
-                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
-                    if (neg == (v + 0) / NM) x.x = -x.x;
-                    if (neg == (v + 1) / NM) x.y = -x.y;
-                    if (neg == (v + 2) / NM) x.z = -x.z;
-                    if (neg == (v + 3) / NM) x.w = -x.w;
-                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
-                }
-            }
-        } else {
-            for (int v = 0; v < 4 * NM; v += 4)
-                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        sk[slot] = kd;
-    }
-    __syncthreads();
-
-    // 1. interface fluxes of the tile, once each
     constexpr int NXF = MTY * (MTX + 1), NYF = (MTY + 1) * MTX;
-    for (int f = tid; f < NXF + NYF; f += MNT) {
+    for (int f = tid; f < NXF + NYF; f += NTHREAD) {
         int sl, sr, side_l, side_r;
         float* dst;
         int dstride;
@@ -412,6 +339,92 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
             for (int c = 0; c < 4; ++c) dst[(q * 4 + c) * dstride] = Fq[c];
         }
     }
+}
+
+// One tile whose top-left cell is (i0, j0), shared memory at `smem`
+// (smem_bytes<P, MTY>()).  Per-thread returns leave only this function: every
+// barrier of the tile precedes them.  LAM (FP64 output only): returns the max
+// corner wave speed of the thread's cell if it is fluid (computeMaxSpeedDG_omp
+// on the FP64 values written), else 0.
+template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
+__device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, float* smem) {
+    constexpr int MNT = MTX * MTY, SY = MTY + 2;
+    constexpr int NQ = P + 1, NM = NQ * NQ;
+    constexpr int SD = SX * SY;  // cell slots of the tile + halo
+    constexpr int VP = vpitch(NM);  // floats per slot: 4*NM padded so 16-byte loads are conflict-free
+    const DGSepF& S = c_sepf[P - 1];
+    float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
+    float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
+    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
+
+    const int tid = threadIdx.x;
+    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
+    const size_t plane = a.g.plane;
+
+    // U^n of this thread's cell is read again only by the combine: start
+    // bringing it into L2 now so those loads overlap the flux work
+    {
+        const int pr = tid / MTX, pc = tid - pr * MTX;
+        if (i0 + pr < ny && j0 + pc < nx) {
+            const double* u0 = a.un + (size_t)(i0 + pr) * pitch + (j0 + pc);
+#pragma unroll 8
+            for (int v = 0; v < 4 * NM; ++v)
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(u0 + (size_t)v * plane));
+        }
+    }
+
+    // 0. gather tile + halo (corners unused)
+    for (int slot = tid; slot < SD; slot += MNT) {
+        const int r = slot / SX, c = slot - r * SX;
+        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        uint8_t kd = KIND_PASSIVE;
+        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+            const size_t k = (size_t)gi * pitch + gj;
+            kd = a.kind[k] & KIND_MASK;
+            size_t ks = k;
+            int neg = -1;
+            if (kd >= KIND_COPY) {
+                ks = (size_t)a.gsrc[k];
+                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
+            }
+            if (sizeof(TIn) == 4) {
+                // FP32 input: asynchronous 4-byte copies, all in flight at once
+                const float* src = static_cast<const float*>(a.cur) + ks;
+#pragma unroll 8
+                for (int v = 0; v < 4 * NM; ++v) {
+                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
+                                 : "memory");
+                }
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                if (neg >= 0)
+                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
+            } else {
+#pragma unroll 4
+                for (int v = 0; v < 4 * NM; v += 4) {
+                    float4 x;
+                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
+                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
+                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
+                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
+                    if (neg == (v + 0) / NM) x.x = -x.x;
+                    if (neg == (v + 1) / NM) x.y = -x.y;
+                    if (neg == (v + 2) / NM) x.z = -x.z;
+                    if (neg == (v + 3) / NM) x.w = -x.w;
+                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
+                }
+            }
+        } else {
+            for (int v = 0; v < 4 * NM; v += 4)
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        sk[slot] = kd;
+    }
+    __syncthreads();
+
+    // 1. interface fluxes of the tile, once each
+    tile_face_fluxes<P, MTY, MNT>(a, sd, sfx, sfy, sk, tid);
     __syncthreads();
 
     // 2. one thread per cell
@@ -841,101 +854,9 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     }
     __syncthreads();
 
-    // 1. interface fluxes, one face per lane pair; the trip count is the same
-    //    for every lane (idle pairs take the last face and store nothing)
-    constexpr int NXF = MTY * (MTX + 1), NYF = (MTY + 1) * MTX, NF = NXF + NYF;
-    for (int base = 0; base < NF; base += MNT) {
-        const int f0 = base + ci;
-        const int f = f0 < NF ? f0 : NF - 1;
-        int sl, sr;
-        float* dst;
-        int dstride;
-        bool ydir;
-        if (f < NXF) {
-            const int r = f / (MTX + 1), c = f - r * (MTX + 1);
-            sl = (r + 1) * SX + c;
-            sr = sl + 1;
-            dst = sfx + r * (MTX + 1) + c;
-            dstride = MTY * (MTX + 1);
-            ydir = false;
-        } else {
-            const int g = f - NXF, r = g / MTX, c = g - r * MTX;
-            sl = r * SX + c + 1;
-            sr = sl + SX;
-            dst = sfy + r * MTX + c;
-            dstride = (MTY + 1) * MTX;
-            ydir = true;
-        }
-        const bool store = f0 < NF && (sk[sl] == KIND_UPDATED || sk[sr] == KIND_UPDATED);
-        float el[2][NQ], er[2][NQ];
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc)
-#pragma unroll
-            for (int n = 0; n < NQ; ++n) el[cc][n] = er[cc][n] = 0.0f;
-        const float* pl = sd + sl * VP + 2 * h * NM;
-        const float* pr = sd + sr * VP + 2 * h * NM;
-        if (ydir) {
-#pragma unroll
-            for (int v = 0; v < 2 * NM; v += VW) {
-                float lv[VW], rv[VW];
-                load_vec<VW>(pl + v, lv);
-                load_vec<VW>(pr + v, rv);
-#pragma unroll
-                for (int e = 0; e < VW; ++e) {
-                    const int cc = (v + e) / NM, m = (v + e) % NM, px = m / NQ, py = m % NQ;
-                    el[cc][px] += lv[e];
-                    er[cc][px] += (py & 1) ? -rv[e] : rv[e];
-                }
-            }
-        } else {
-#pragma unroll
-            for (int v = 0; v < 2 * NM; v += VW) {
-                float lv[VW], rv[VW];
-                load_vec<VW>(pl + v, lv);
-                load_vec<VW>(pr + v, rv);
-#pragma unroll
-                for (int e = 0; e < VW; ++e) {
-                    const int cc = (v + e) / NM, m = (v + e) % NM, px = m / NQ, py = m % NQ;
-                    el[cc][py] += lv[e];
-                    er[cc][py] += (px & 1) ? -rv[e] : rv[e];
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            float ul[2], ur[2];
-#pragma unroll
-            for (int cc = 0; cc < 2; ++cc) {
-                float x = 0.0f, y = 0.0f;
-#pragma unroll
-                for (int n = 0; n < NQ; ++n) {
-                    x = fmaf(el[cc][n], S.L[n][q], x);
-                    y = fmaf(er[cc][n], S.L[n][q], y);
-                }
-                ul[cc] = x;
-                ur[cc] = y;
-            }
-            float UL[4], UR[4];
-            join_pair(h, ul[0], ul[1], __shfl_xor_sync(FULL, ul[0], 1), __shfl_xor_sync(FULL, ul[1], 1), UL);
-            join_pair(h, ur[0], ur[1], __shfl_xor_sync(FULL, ur[0], 1), __shfl_xor_sync(FULL, ur[1], 1), UR);
-            float Fq[4];
-            if (ydir) {
-                float l[4] = {UL[0], UL[2], UL[1], UL[3]};
-                float r[4] = {UR[0], UR[2], UR[1], UR[3]};
-                float g[4];
-                if (a.hll) hlle_dg_f(l, r, a.gamma, g);
-                else hllc_dg_f(l, r, a.gamma, g);
-                Fq[0] = g[0]; Fq[1] = g[2]; Fq[2] = g[1]; Fq[3] = g[3];
-            } else {
-                if (a.hll) hlle_dg_f(UL, UR, a.gamma, Fq);
-                else hllc_dg_f(UL, UR, a.gamma, Fq);
-            }
-            if (store) {
-                dst[(q * 4 + 2 * h) * dstride] = h ? Fq[2] : Fq[0];
-                dst[(q * 4 + 2 * h + 1) * dstride] = h ? Fq[3] : Fq[1];
-            }
-        }
-    }
+    // 1. interface fluxes: one thread per face (all four variables), so no
+    //    flux is evaluated twice and the 256 threads cover the faces in two rounds
+    tile_face_fluxes<P, MTY, NT>(a, sd, sfx, sfy, sk, tid);
     __syncthreads();
 
     // 2. one lane pair per cell
