@@ -1210,8 +1210,8 @@ __global__ void __launch_bounds__(MTX * 4, P == 1 ? 8 : 3) dg_stage_mixed_kernel
 
 // The same stage with two threads per cell (stage_tile_pair).  Register
 // shares: 1024 threads per SM for P = 1, 768 for P = 2 (80 registers, no
-// spills), 512 for P = 3 (2 CTAs of 8 warps at 128 registers; 768 spilled 300
-// bytes and ran 17% slower).
+// spills; 512 ran 15% slower), 512 for P = 3 (2 CTAs of 8 warps at 128
+// registers; 768 spilled and ran 17% slower).
 constexpr int pair_thread_budget(int P) { return P == 1 ? 1024 : P == 3 ? 512 : 768; }
 // Tile rows of the single-problem two-threads-per-cell kernel: 32 x 2 tiles (4
 // CTAs of 128 threads, the same 16 warps per SM) ran 9% slower at P = 3 (the
@@ -1228,9 +1228,9 @@ __global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P>()) dg_
 }
 
 // Threads per cell of the single-problem stage kernel, per P (measured at
-// 2048^2, four-quadrant, GDOF/s): P = 1 34.2 (one) vs 26.5 (two), P = 2 37.2
-// vs 33.4, P = 3 29.7-30.3 vs 31.1.
-constexpr int kSingleTpc[4] = {0, 1, 1, 2};
+// 2048^2, four-quadrant, GDOF/s, one vs two threads per cell): P = 1 38.4 vs
+// 35.9, P = 2 39.0 vs 42.5, P = 3 33.8 vs 39.0.
+constexpr int kSingleTpc[4] = {0, 1, 2, 2};
 
 // Persistent stage STAGE over every listed problem of a batch group, tile
 // variant V (dg_variant_rows(V) rows, dg_variant_tpc(V) threads per cell):
