@@ -425,15 +425,16 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
 
     // 1. interface fluxes of the tile, once each
     tile_face_fluxes<P, MTY, MNT>(a, sd, sfx, sfy, sk, tid);
-    __syncthreads();
+    // no barrier yet: the volume quadrature reads only the gathered state, so
+    // threads without a last-round face start on it while the last faces finish
 
     // 2. one thread per cell
     const int r = tid / MTX, c = tid - r * MTX;
     const int gi = i0 + r, gj = j0 + c;
-    if (gi >= ny || gj >= nx) return 0.0;
+    const bool inside = gi < ny && gj < nx;
     const int slot = (r + 1) * SX + c + 1;
-    const size_t k = (size_t)gi * pitch + gj;
-    const uint8_t kd = sk[slot];
+    const size_t k = inside ? (size_t)gi * pitch + gj : 0;
+    const uint8_t kd = inside ? sk[slot] : (uint8_t)KIND_PASSIVE;
     float acc[4][NM];
 #pragma unroll
     for (int q = 0; q < 4; ++q)
@@ -500,6 +501,10 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
                         acc[c][px * NQ + py] = fmaf(dx, f[c][py], fmaf(lx, g[c][py], acc[c][px * NQ + py]));
             }
         }
+    }
+    __syncthreads();  // every interface flux is in shared memory
+    if (!inside) return 0.0;
+    if (kd == KIND_UPDATED) {
         // face integrals (src_DG/fluid.cpp:731-796): right (-) and left (+) x
         // faces weigh the face-normal factor P_px(+1) = 1 and P_px(-1) =
         // (-1)^px; bottom (-) and top (+) y faces P_py(+-1).  h = sum_q w_q
@@ -857,18 +862,18 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     // 1. interface fluxes: one thread per face (all four variables), so no
     //    flux is evaluated twice and the 256 threads cover the faces in two rounds
     tile_face_fluxes<P, MTY, NT>(a, sd, sfx, sfy, sk, tid);
-    __syncthreads();
+    // no barrier yet: the volume quadrature reads only the gathered state, so
+    // warps without a second face start on it while the last faces finish
 
     // 2. one lane pair per cell
     const int r = ci / MTX, c = ci - r * MTX;
     const int gi = i0 + r, gj = j0 + c;
     const bool inside = gi < ny && gj < nx;
     const unsigned pm = __ballot_sync(FULL, inside);  // lanes of cells in the grid (whole pairs)
-    if (!inside) return 0.0;
     const int slot = (r + 1) * SX + c + 1;
-    const size_t k = (size_t)gi * pitch + gj;
-    const uint8_t kd = sk[slot];
-    const unsigned um = __ballot_sync(pm, kd == KIND_UPDATED);
+    const size_t k = inside ? (size_t)gi * pitch + gj : 0;
+    const uint8_t kd = inside ? sk[slot] : (uint8_t)KIND_PASSIVE;
+    const unsigned um = __ballot_sync(FULL, kd == KIND_UPDATED);
     float acc[2][NM];
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc)
@@ -935,6 +940,10 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                         acc[cc][px * NQ + py] = fmaf(dx, f[cc][py], fmaf(lx, g[cc][py], acc[cc][px * NQ + py]));
             }
         }
+    }
+    __syncthreads();  // every interface flux is in shared memory
+    if (!inside) return 0.0;
+    if (kd == KIND_UPDATED) {
         // face integrals of this half's variables (order of stage_tile)
         {
             const float* Fr = sfx + r * (MTX + 1) + c + 1;
