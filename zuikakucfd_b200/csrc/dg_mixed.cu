@@ -401,7 +401,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
                 if (neg >= 0)
                     for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
             } else {
-#pragma unroll 4
+#pragma unroll 8
                 for (int v = 0; v < 4 * NM; v += 4) {
                     float4 x;
                     x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
@@ -837,7 +837,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                 if (neg >= 0)
                     for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
             } else {
-#pragma unroll 4
+#pragma unroll 8
                 for (int v = 0; v < 4 * NM; v += 4) {
                     float4 x;
                     x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
