@@ -136,6 +136,37 @@ int zk_step_timed(zk_ctx* ctx, double dt, int nsteps, float* ms);
  * doubles) and its row pitch in elements, for zero-copy callers. */
 int zk_state_device(zk_ctx* ctx, double** dptr, int* pitch);
 
+/* ---- x-slab decomposition ----------------------------------------------------
+ * A grid split into x-slabs, one context (and one GPU) each, as the
+ * reference's MPI runs split it (splitMeshVertically, src_WENO/fluid.cpp:99-152):
+ * every inner slab side carries 3 exchange columns (bctype -3, boundary
+ * ZK_BOUNDARY_EXCHANGE), which a stage reads as stored and never updates.
+ * One step of a slab is, for stage = 1, 2, 3:
+ *   zk_stage(stage); [DG TVB limiters: exchange(stage); zk_stage_limit(stage);]
+ *   exchange(stage)
+ * where exchange(stage) sends the 3 owned columns next to each inner side to
+ * the neighbour and stores the 3 columns received in the exchange columns --
+ * exchangeConservativeColumns after every stage and limiter pass
+ * (src_WENO/fluid.cpp:160-198, 468-493; src_DG/fluid.cpp:342-400, 1005-1054).
+ * The owned cells of the slabs then hold the bits one context over the whole
+ * grid computes.  All of these only enqueue work on the context's stream. */
+/* Stage 1, 2 or 3 of one zk_step (the same kernels; the DG reference limiter
+ * is part of the stage).  Stage 1 clears the status word and the limited-cell
+ * count, as zk_step does. */
+int zk_stage(zk_ctx* ctx, double dt, int stage);
+/* The TVB pass zk_step runs after `stage` (DG TVB limiters; no-op otherwise). */
+int zk_stage_limit(zk_ctx* ctx, int stage);
+/* Halo of the state written by `stage` (0 or 3: U^n; 1, 2: the stage states):
+ * nplanes x ny x 3 elements (FP32 for the stage states of a mixed-precision
+ * DG context, else FP64), buffer layout [plane][row][column].  side 0 = left,
+ * 1 = right.  zk_halo_pack copies the 3 owned columns next to that side
+ * (3..5, or nx-6..nx-4) into dev_buf; zk_halo_unpack copies dev_buf into the
+ * exchange columns of that side (0..2, or nx-3..nx-1).  dev_buf is device
+ * memory of at least zk_halo_bytes bytes on the context's device. */
+int zk_halo_bytes(zk_ctx* ctx, int stage, size_t* bytes);
+int zk_halo_pack(zk_ctx* ctx, int stage, int side, void* dev_buf);
+int zk_halo_unpack(zk_ctx* ctx, int stage, int side, const void* dev_buf);
+
 /* ---- learned troubled-cell indicator (no counterpart in the reference) ----
  * A 40 -> 32 -> 32 -> 32 -> 1 GELU MLP gates the TVB limiter of
  * ZK_LIMITER_TVB_MLP contexts: only cells with a positive logit take the

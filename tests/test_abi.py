@@ -55,6 +55,20 @@ def test_default_options_and_errors_without_device(lib):
     assert lib.zk_version() >= 100
 
 
+
+def test_slab_entry_points_reject_a_null_context(lib):
+    """zk_stage / zk_halo_* check their context before any device work."""
+    lib.zk_last_error.restype = C.c_char_p
+    n = C.c_size_t()
+    lib.zk_stage.argtypes = [C.c_void_p, C.c_double, C.c_int]
+    assert lib.zk_stage(None, C.c_double(1e-3), 1) == 1
+    assert lib.zk_stage_limit(None, 1) == 1
+    assert lib.zk_halo_bytes(None, 0, C.byref(n)) == 1
+    assert lib.zk_halo_pack(None, 0, 0, None) == 1
+    assert lib.zk_halo_unpack(None, 0, 1, None) == 1
+    assert b"null context" in lib.zk_last_error()
+
+
 def test_batch_default_options_and_bad_options(lib):
     """Batch defaults (tuned WENO tile, 10 graph steps) and option checks that
     run before any device work."""

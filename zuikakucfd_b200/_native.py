@@ -102,6 +102,11 @@ _SIGS = {
                                        C.POINTER(C.c_int32), C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_uint32)]),
     "zk_mach_number": (C.c_int, [_P, _D, _D]),
+    "zk_stage": (C.c_int, [_P, C.c_double, C.c_int]),
+    "zk_stage_limit": (C.c_int, [_P, C.c_int]),
+    "zk_halo_bytes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_size_t)]),
+    "zk_halo_pack": (C.c_int, [_P, C.c_int, C.c_int, _P]),
+    "zk_halo_unpack": (C.c_int, [_P, C.c_int, C.c_int, _P]),
     "zk_batch_default_options": (None, [C.POINTER(zk_batch_options)]),
     "zk_batch_create": (C.c_int, [C.POINTER(zk_batch_options), C.POINTER(_P)]),
     "zk_batch_add": (C.c_int, [_P, C.POINTER(zk_options), C.c_int, C.c_int, C.c_double, C.c_double,

@@ -44,6 +44,7 @@ SOURCES: list[tuple[str, list[str]]] = [
     ("peak.cu", []),
     ("weno_mixed.cu", ["--use_fast_math"]),
     ("noalloc.cu", []),
+    ("slab.cu", []),
     ("batch.cu", []),
 ]
 

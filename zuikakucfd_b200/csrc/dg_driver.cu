@@ -155,6 +155,35 @@ int zk_dg_step(zk_ctx* c, double dt) {
     return zk_dg_after_stage(c, c->Un, true);
 }
 
+// Stage `stage` (1..3) of zk_dg_step alone, without the TVB pass after it:
+// the same launch with the same buffers (FP64: U^n -> S1 -> S2 -> U^n;
+// mixed: U^n -> F1 -> F2 -> U^n).
+int zk_dg_stage(zk_ctx* c, double dt, int stage) {
+    const int P = c->opt.order;
+    cudaError_t e;
+    if (c->opt.precision == ZK_PREC_MIXED) {
+        const void* in = stage == 1 ? (const void*)c->Un : (const void*)(stage == 2 ? c->F1 : c->F2);
+        void* out = stage == 3 ? (void*)c->Un : (void*)(stage == 1 ? c->F1 : c->F2);
+        e = zk::launch_dg_stage_mixed(P, in, stage == 1, c->Un, out, stage == 3, c->kind, c->gsrc, c->g, dt, c->da,
+                                      c->gamma, stage, c->opt.limiter, c->opt.flux == ZK_FLUX_HLL, st(c)->s0,
+                                      c->d_status, c->stream);
+    } else {
+        double* in[3] = {c->Un, c->S1, c->S2};
+        double* out[3] = {c->S1, c->S2, c->Un};
+        e = zk::launch_dg_stage_fp64(P, args(c, in[stage - 1], c->Un, out[stage - 1], dt, stage), c->stream);
+    }
+    return e == cudaSuccess ? ZK_OK : cuda_fail(e);
+}
+
+// The TVB pass zk_dg_step runs after stage `stage` (nothing for the other
+// limiters), on that stage's output.
+int zk_dg_stage_limit(zk_ctx* c, int stage) {
+    if (c->opt.precision == ZK_PREC_MIXED)
+        return stage == 3 ? zk_dg_after_stage(c, c->Un, true) : zk_dg_after_stage(c, stage == 1 ? c->F1 : c->F2, false);
+    double* out[3] = {c->S1, c->S2, c->Un};
+    return zk_dg_after_stage(c, out[stage - 1], true);
+}
+
 int zk_dg_rhs(zk_ctx* c, double* dU_dev) {
     cudaError_t e = zk::launch_dg_stage_fp64(c->opt.order, args(c, c->Un, c->Un, dU_dev, 0.0, 0), c->stream);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);

@@ -529,3 +529,15 @@ int zk_weno_mixed_step(zk_ctx* c, double dt) {
     if (e != cudaSuccess) return zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
     return ZK_OK;
 }
+
+// Stage `stage` (1..3) of zk_weno_mixed_step alone: the same launch with the
+// same buffers (U^n -> S1 -> S2 -> U^n).
+int zk_weno_mixed_stage(zk_ctx* c, double dt, int stage) {
+    const double dtdx = dt / c->da, dtdy = dt / c->da;
+    double* in[3] = {c->Un, c->S1, c->S2};
+    double* out[3] = {c->S1, c->S2, c->Un};
+    const cudaError_t e = zk::launch_weno_stage_mixed(c->tmap[stage - 1], in[stage - 1], c->Un, out[stage - 1], c->kind,
+                                                      c->gsrc, c->g, dtdx, dtdy, c->gamma, stage, c->d_status,
+                                                      c->stream);
+    return e == cudaSuccess ? ZK_OK : zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
+}

@@ -59,7 +59,10 @@ int zk_dg_step(zk_ctx* c, double dt);
 int zk_dg_rhs(zk_ctx* c, double* dU_dev);
 int zk_dg_limit(zk_ctx* c);
 int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64);
+int zk_dg_stage(zk_ctx* c, double dt, int stage);
+int zk_dg_stage_limit(zk_ctx* c, int stage);
 
 // WENO mixed-precision driver (weno_mixed.cu)
 int zk_weno_mixed_setup(zk_ctx* c);
 int zk_weno_mixed_step(zk_ctx* c, double dt);
+int zk_weno_mixed_stage(zk_ctx* c, double dt, int stage);

@@ -47,6 +47,7 @@ class Solver:
         N.check(L.zk_create(C.byref(o), C.byref(h)))
         self._h = h
         self.method, self.order, self.precision = method, int(order), precision
+        self.limiter, self.device = limiter, int(device)
         self.nm = (self.order + 1) ** 2 if method == "dg" else 1
         self.ny = self.nx = 0
 
@@ -136,6 +137,39 @@ class Solver:
 
     def set_stream(self, stream_handle: int | None) -> None:
         N.check(N.lib().zk_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    # -- one stage at a time and slab halos (zuikakucfd_b200.slab) ------------------
+    def stage(self, dt: float, stage: int) -> None:
+        """Enqueue stage 1, 2 or 3 of one step (the kernels zk_step runs)."""
+        N.check(N.lib().zk_stage(self._h, float(dt), int(stage)))
+
+    def stage_limit(self, stage: int) -> None:
+        """Enqueue the TVB pass that follows `stage` (no-op for other limiters)."""
+        N.check(N.lib().zk_stage_limit(self._h, int(stage)))
+
+    def halo_bytes(self, stage: int) -> int:
+        v = C.c_size_t()
+        N.check(N.lib().zk_halo_bytes(self._h, int(stage), C.byref(v)))
+        return int(v.value)
+
+    def halo_pack(self, stage: int, side: int, buf) -> None:
+        """Copy the 3 owned columns next to `side` (0 left, 1 right) of the
+        state `stage` wrote into `buf`, a device tensor on this context's
+        device of at least halo_bytes(stage) bytes."""
+        N.check(N.lib().zk_halo_pack(self._h, int(stage), int(side), C.c_void_p(_device_ptr(buf, self.device))))
+
+    def halo_unpack(self, stage: int, side: int, buf) -> None:
+        """Store `buf` (as packed by the neighbour) in the exchange columns of `side`."""
+        N.check(N.lib().zk_halo_unpack(self._h, int(stage), int(side), C.c_void_p(_device_ptr(buf, self.device))))
+
+
+def _device_ptr(buf, device: int) -> int:
+    """Address of a CUDA tensor on `device`; anything else is refused, since
+    the halo kernels dereference it on the GPU."""
+    dev = getattr(buf, "device", None)
+    if dev is None or dev.type != "cuda" or dev.index != device:
+        raise ValueError(f"halo buffer must be a CUDA tensor on cuda:{device}")
+    return int(buf.data_ptr())
 
 
 # ---------------------------------------------------------------------------------
@@ -292,11 +326,63 @@ def computeRHS(mesh: Mesh, dt: float) -> np.ndarray:
 
 def updateMesh(mesh: Mesh, dt: float, rank: int = 0, num_procs: int = 1) -> None:
     """One SSP-RK3 step in place (src_WENO/fluid.cpp:468-493,
-    src_DG/fluid.cpp:1005-1054).  One device owns the whole grid, so rank and
-    num_procs must be 0 and 1 (the reference's MPI slab split is not used)."""
-    if num_procs != 1 or rank != 0:
-        raise ValueError("updateMesh on the GPU takes the whole grid: rank=0, num_procs=1")
-    mesh.solver().step(dt, 1)
+    src_DG/fluid.cpp:1005-1054).  With num_procs > 1, ``mesh`` is this rank's
+    slab from splitMeshVertically and the step runs stage by stage with the
+    exchange of its 3-column halos after every stage (and DG TVB pass) over the
+    default torch.distributed group, whose ranks all call updateMesh."""
+    if num_procs == 1:
+        if rank != 0:
+            raise ValueError("one process: rank must be 0")
+        mesh.solver().step(dt, 1)
+    else:
+        from . import slab
+        s = mesh.solver()
+        slab.slab_step([s], _slab_exchange(mesh, rank, num_procs), dt, 1)
+        s.synchronize()
+    mesh._device_changed()
+
+
+def splitMeshVertically(original: Mesh, n: int) -> list[Mesh]:
+    """splitMeshVertically (src_WENO/fluid.cpp:99-152, src_DG/fluid.cpp:249-312):
+    n x-slab Meshes.  Slab k owns widths[k] = remain // (n - k) columns and has
+    3 exchange columns (bctype -3) on every inner side, filled from the
+    neighbour's columns; primitives, the conserved state (all DG modes) and
+    bctype are copied.  Every slab needs at least 6 owned columns."""
+    from . import slab
+    prim = np.stack([original.rho, original.u, original.v, original.p])
+    state_parts = slab.split_arrays(original.state, original.bctype, n)
+    prim_parts = slab.split_arrays(prim, original.bctype, n)
+    out = []
+    for (st, b), (pr, _) in zip(state_parts, prim_parts):
+        m = Mesh(original.ny, b.shape[1], original.da, original.gamma, **original._opts)
+        m.bctype = b
+        m.rho, m.u, m.v, m.p = (pr[c].copy() for c in range(4))
+        m.state = st
+        out.append(m)
+    return out
+
+
+def _slab_exchange(mesh: Mesh, rank: int, num_procs: int):
+    from . import slab
+    if not 0 <= rank < num_procs:
+        raise ValueError(f"rank {rank} outside 0..{num_procs - 1}")
+    ex = getattr(mesh, "_exchange", None)
+    if ex is None or ex.solver is not mesh.solver() or (ex.rank, ex.nprocs) != (rank, num_procs):
+        ex = slab.DistExchange(mesh.solver(), rank, num_procs)
+        mesh._exchange = ex
+    return ex
+
+
+def exchangeConservativeColumns(mesh: Mesh, rank: int, num_procs: int) -> None:
+    """exchangeConservativeColumns (src_WENO/fluid.cpp:192-198,
+    src_DG/fluid.cpp:342-400): this rank's slab swaps the 3 columns next to
+    each inner side, all variables and DG modes, with ranks rank-1 and rank+1
+    of the default torch.distributed group."""
+    if num_procs == 1:
+        return
+    s = mesh.solver()
+    _slab_exchange(mesh, rank, num_procs)(0)
+    s.synchronize()
     mesh._device_changed()
 
 
