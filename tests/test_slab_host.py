@@ -62,6 +62,18 @@ def test_split_mesh_vertically_copies_fields_and_options():
     assert np.array_equal(slab.join_arrays([s.state for s in subs], 50), m.state)
 
 
+def test_slab_calls_check_the_rank_before_any_device_work():
+    from zuikakucfd_b200 import Mesh, exchangeConservativeColumns, updateMesh
+    m = Mesh(12, 20, 0.05, 1.4)
+    for rank, n in [(1, 1), (2, 2), (-1, 3)]:
+        with pytest.raises(ValueError):
+            updateMesh(m, 1e-3, rank, n)
+        with pytest.raises(ValueError):
+            exchangeConservativeColumns(m, rank, n)
+    exchangeConservativeColumns(m, 0, 1)  # one rank: nothing to exchange
+    assert m._solver is None
+
+
 class HostSlab:
     """Stand-in for a device context on the host: a nonlinear 7-point x
     stencil updates columns [3, nx-3) in each SSP-RK3 stage, exchange and

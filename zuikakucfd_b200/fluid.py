@@ -330,9 +330,9 @@ def updateMesh(mesh: Mesh, dt: float, rank: int = 0, num_procs: int = 1) -> None
     slab from splitMeshVertically and the step runs stage by stage with the
     exchange of its 3-column halos after every stage (and DG TVB pass) over the
     default torch.distributed group, whose ranks all call updateMesh."""
+    if not 0 <= rank < num_procs:
+        raise ValueError(f"rank {rank} outside 0..{num_procs - 1}")
     if num_procs == 1:
-        if rank != 0:
-            raise ValueError("one process: rank must be 0")
         mesh.solver().step(dt, 1)
     else:
         from . import slab
@@ -378,6 +378,8 @@ def exchangeConservativeColumns(mesh: Mesh, rank: int, num_procs: int) -> None:
     src_DG/fluid.cpp:342-400): this rank's slab swaps the 3 columns next to
     each inner side, all variables and DG modes, with ranks rank-1 and rank+1
     of the default torch.distributed group."""
+    if not 0 <= rank < num_procs:
+        raise ValueError(f"rank {rank} outside 0..{num_procs - 1}")
     if num_procs == 1:
         return
     s = mesh.solver()
