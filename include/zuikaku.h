@@ -120,7 +120,8 @@ int zk_recover_primitives(zk_ctx* ctx, double* host_prim);
 int zk_mach_number(zk_ctx* ctx, double* host_mach, double* host_speed);
 
 /* Device status word (bit 0: NaN seen, bit 1: rho <= 0, bit 2: p <= 0) of the
- * last zk_step; cleared by each zk_step. */
+ * last zk_step, or of the zk_stage calls since the last stage 1; cleared by
+ * each zk_step and each zk_stage(ctx, dt, 1). */
 int zk_status_word(zk_ctx* ctx, uint32_t* out);
 
 /* Stream control: run on an external stream (e.g. one owned by a framework)
