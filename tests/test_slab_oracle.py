@@ -28,11 +28,12 @@ def _case(order=0, seed=7):
     return c, d, 0.5 * 0.9 / (2.0 * (2 * order + 1)) * c.da / lam
 
 
-def _exchange(parts):
-    """exchangeColumns between neighbouring slabs, in place."""
+def _exchange(parts, width=3):
+    """exchangeColumns between neighbouring slabs, in place: the `width`
+    exchange columns nearest the owned cells (3 in the reference)."""
     for a, b in zip(parts, parts[1:]):
-        b[..., 0:3] = a[..., -6:-3]
-        a[..., -3:] = b[..., 3:6]
+        b[..., 3 - width:3] = a[..., -3 - width:-3]
+        a[..., -3:-3 + width if width < 3 else None] = b[..., 3:3 + width]
 
 
 def _combine(k, un, cur, inc):
@@ -57,7 +58,7 @@ def _weno_steps(rs, parts, bcts, c, dt, nsteps, exchange=True):
     return parts
 
 
-def _dg_steps(rs, P, parts, bcts, c, dt, nsteps, limiter):
+def _dg_steps(rs, P, parts, bcts, c, dt, nsteps, limiter, width=3):
     for _ in range(nsteps):
         dn = [d.copy() for d in parts]
         for k in (1, 2, 3):
@@ -69,9 +70,9 @@ def _dg_steps(rs, P, parts, bcts, c, dt, nsteps, limiter):
             if limiter == "reference":
                 parts = [rs.dg_limit(P, d, b, c.gamma) for d, b in zip(parts, bcts)]
             else:  # TVB reads the neighbours' means: exchange, limit, exchange
-                _exchange(parts)
+                _exchange(parts, width)
                 parts = [rs.dg_limit_tvb(P, d, b, c.da, c.gamma)[0] for d, b in zip(parts, bcts)]
-            _exchange(parts)
+            _exchange(parts, width)
     return parts
 
 
@@ -95,3 +96,28 @@ def test_dg_slabs_match_the_whole_grid_step(restatement, P, limiter):
     split = slab.split_arrays(d, c.bctype, 3)
     got = _dg_steps(restatement, P, [s for s, _ in split], [b for _, b in split], c, dt, 2, limiter)
     assert np.array_equal(slab.join_arrays(got, c.nx), whole)
+
+
+@pytest.mark.parametrize("limiter", ["reference", "tvb"])
+def test_dg_needs_one_exchange_column(restatement, limiter):
+    """DG reads only the face neighbour across a slab side (face fluxes and
+    the TVB neighbour means), so exchanging the innermost column alone gives
+    the same bits -- a third of the reference's halo bytes.  WENO's 6-point
+    stencils need all three."""
+    c, d, dt = _case(2)
+    whole = restatement.dg_step_lim(2, d, c.bctype, c.da, c.gamma, dt, nsteps=2, limiter=limiter)
+    split = slab.split_arrays(d, c.bctype, 3)
+    got = _dg_steps(restatement, 2, [s for s, _ in split], [b for _, b in split], c, dt, 2, limiter, width=1)
+    assert np.array_equal(slab.join_arrays(got, c.nx), whole)
+    c, U, dt = _case()
+    whole = restatement.weno_step(U, c.bctype, c.da, c.gamma, dt, nsteps=2)
+    split = slab.split_arrays(U, c.bctype, 3)
+    parts = [s_.copy() for s_, _ in split]
+    for _ in range(2):
+        un = [u.copy() for u in parts]
+        for k in (1, 2, 3):
+            parts = [_combine(k, n0, *rs_out) for n0, rs_out in
+                     zip(un, (restatement.weno_rhs(u, b, c.da, c.gamma, dt) for u, (_, b) in zip(parts, split)))]
+            _exchange(parts, 2)
+    assert not np.array_equal(slab.join_arrays(parts, c.nx), whole)
+
