@@ -88,7 +88,8 @@ def test_weno_slabs_match_the_whole_grid_step(restatement):
     assert not np.array_equal(slab.join_arrays(stale, c.nx), whole)
 
 
-@pytest.mark.parametrize("P,limiter", [(1, "reference"), (2, "reference"), (2, "tvb")])
+@pytest.mark.parametrize("P,limiter", [(1, "reference"), (2, "reference"), (2, "tvb"), (3, "reference"),
+                                       (3, "tvb")])
 def test_dg_slabs_match_the_whole_grid_step(restatement, P, limiter):
     c, d, dt = _case(P)
     whole = restatement.dg_step_lim(P, d, c.bctype, c.da, c.gamma, dt, nsteps=2, limiter=limiter)
