@@ -228,7 +228,8 @@ def cpu_baseline(w: dict, seconds: float = 15.0) -> dict:
     v = cells * w["dof_per_cell"] * n / (ms * 1e-3)
     return {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"{n} x updateMesh on a {rows}x{c.nx} strip of the {c.ny}x{c.nx} grid split into "
-                      f"{cores} x-slabs (one thread per slab, reference Makefile flags, halo exchange omitted)",
+                      f"{cores} x-slabs (one thread per slab, reference Makefile flags at ISA {R.isa}, "
+                      "halo exchange omitted)",
             "ms": ms}
 
 
@@ -245,7 +246,7 @@ def run_reference_arm(args, w) -> dict:
     ms, cells = _ref_slabs(R, w, st, b, args.steps, cores)
     v = cells * w["dof_per_cell"] * args.steps / (ms * 1e-3)
     sample = (f"{rows}x{c.nx} strip of the {c.ny}x{c.nx} grid per step, {cores} x-slab threads, "
-              f"reference Makefile flags")
+              f"reference Makefile flags at ISA {R.isa}")
     return {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -299,6 +300,12 @@ def main():
         args.warmup = 3
 
     rank, world, local, pg = dist_setup(args.gpus)
+    if args.workload.startswith("slab"):
+        if rank == 0 and args.impl == "ours":
+            print(json.dumps(run_slab(args)), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
     if args.workload.startswith("batch"):
         if args.impl == "reference":
             if rank == 0:
@@ -435,7 +442,7 @@ def batch_cpu_rates(seconds: float = 8.0) -> dict:
         n = max(1, int(seconds * 1e3 / max(ms, 1.0)))
         ms, cells = _ref_slabs(R, w, st, b, n, cores)
         out[key] = ms * 1e-3 / (cells * n)
-        out[key + "_sample"] = f"{n} x updateMesh on a {rows}x1024 strip, {cores} x-slab threads"
+        out[key + "_sample"] = f"{n} x updateMesh on a {rows}x1024 strip, {cores} x-slab threads, ISA {R.isa}"
     return out
 
 
@@ -552,6 +559,68 @@ def run_reference_batch(args) -> dict:
                              "sample": f"WENO5: {r['weno_sample']}; DG P=2: {r['dg2_sample']}; per-cell-step "
                                        "costs applied to the batch's cell-steps"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_slab(args) -> dict:
+    """--workload slab<N>: ms per step of one context over the whole grid
+    (zk_step, CUDA events) against N x-slabs of it on this GPU (LocalExchange,
+    halos exchanged after every stage), and ms per step of the exchanges alone;
+    WENO5 mixed at 2048^2 and DG P=3 mixed at 1024^2, four-quadrant seed 1."""
+    import torch
+    from zuikakucfd_b200 import cases
+    from zuikakucfd_b200.fluid import Solver
+    from zuikakucfd_b200.slab import LocalExchange, slab_step, split_arrays
+    nslab = int(args.workload[len("slab"):] or 2)
+    steps = args.steps
+
+    def one(method, precision, order, n):
+        c = cases.four_quadrant(n, seed=1)
+        U = c.conserved()
+        if method == "dg":
+            st = np.zeros((4, (order + 1) ** 2, c.ny, c.nx))
+            st[:, 0] = U
+            U = st
+            dt = 0.5 * 0.9 / (2.0 * (2 * order + 1)) * cases.cfl_dt(c, 1.0)
+        else:
+            dt = cases.cfl_dt(c, 0.4)
+
+        def make(b, st_):
+            s_ = Solver(method=method, order=order, precision=precision)
+            s_.set_mesh(c.ny, b.shape[1], c.da, c.gamma, b)
+            s_.set_state(st_)
+            return s_
+
+        w = make(c.bctype, U)
+        w.step(dt, args.warmup)
+        ms_whole = w.step_timed(dt, steps) / steps
+        w.close()
+        solvers = [make(b, s_) for s_, b in split_arrays(U, c.bctype, nslab)]
+        try:
+            ex = LocalExchange(solvers)
+            slab_step(solvers, ex, dt, args.warmup)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(ex.stream)
+            slab_step(solvers, ex, dt, steps)
+            e1.record(ex.stream)
+            e1.synchronize()
+            ms_slab = e0.elapsed_time(e1) / steps
+            e0.record(ex.stream)
+            for _ in range(50):
+                for k in (1, 2, 3):
+                    ex(k)
+            e1.record(ex.stream)
+            e1.synchronize()
+            ms_ex = e0.elapsed_time(e1) / 50
+        finally:
+            for s_ in solvers:
+                s_.close()
+        return {"ms_step_whole": ms_whole, f"ms_step_{nslab}slabs_one_gpu": ms_slab, "ms_exchanges_per_step": ms_ex}
+
+    out = {f"{m}_{p}_P{o}_{n}": one(m, p, o, n) for m, p, o, n in [("weno", "mixed", 2, 2048), ("dg", "mixed", 3, 1024)]}
+    return {"workload": args.workload, "slabs": nslab, "steps": steps, "warmup": args.warmup,
+            "what": "x-slab decomposition on one GPU vs the whole grid (a diagnostic line, not the metric)",
+            "results": out}
 
 
 def gpu_launches(w, prec) -> int:

@@ -213,7 +213,9 @@ int zk_peak_flops(int device, int kind, double* tflops);
  * 17.3 MiB held on each GPU that loads it, until exit).  Limit:
  * ny * pitch <= 262144 cells, else ZK_ERR_ARG.  Runs on `stream` (NULL = the
  * default stream) of the current device.  The first call on a device looks up
- * the scratch address and must come before any stream capture.  Calls whose
+ * the scratch address and must come before any stream capture; so must the
+ * first call after that device's context was reset (cudaDeviceReset), which
+ * looks it up again.  Calls whose
  * GPU work overlaps race on the shared scratch.  status_out (host, may be
  * NULL) receives the status word and makes the call synchronous. */
 int zk_weno_step_noalloc(double* state, int ny, int nx, int pitch, double da, double gamma,

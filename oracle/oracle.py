@@ -16,6 +16,7 @@ U[4][ny][nx], dof[4][NM][ny][nx], bctype int32[ny][nx].
 from __future__ import annotations
 
 import ctypes as C
+import os
 import subprocess
 from pathlib import Path
 
@@ -23,6 +24,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
+# Where the reference checkout lies: ZK_REFERENCE_DIR, else the read-only
+# checkout this build was made against.  Only build() and the golden-vector
+# generator read it; built outputs go to _ref/ and travel without it.
+REFERENCE_SOURCES = Path(os.environ.get("ZK_REFERENCE_DIR", "/root/reference"))
 RESTATEMENT = HERE / "_build" / "liboracle.so"
 
 _D = C.POINTER(C.c_double)
@@ -43,12 +48,21 @@ def build(reference: bool = True) -> None:
     """Compile the restatement and, when the reference sources exist, oracle/_ref
     (with the drop-in CLIs once the native library is built)."""
     targets = ["restatement"]
-    if reference and Path("/root/reference/src_WENO/fluid.cpp").exists():
+    if reference and (REFERENCE_SOURCES / "src_WENO" / "fluid.cpp").exists():
         targets.append("ref")
         lib = HERE.parent / "zuikakucfd_b200" / "lib" / "libzuikaku.so"
         if lib.exists():  # the reference CLIs linked against the GPU backend
             targets.append("dropin")
-    subprocess.run(["make", "-s", "-C", str(HERE), "-j8", *targets], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), "-j8", f"REF={REFERENCE_SOURCES}", *targets], check=True)
+
+
+def host_has_avx512() -> bool:
+    """The host CPU implements the x86-64-v4 level (AVX-512 F/BW/CD/DQ/VL)."""
+    try:
+        flags = next(l for l in Path("/proc/cpuinfo").read_text().splitlines() if l.startswith("flags")).split()
+    except (OSError, StopIteration):
+        return False
+    return all(f in flags for f in ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"))
 
 
 def reference_available(variant: str = "faithful") -> bool:
@@ -213,6 +227,11 @@ class Reference:
     def __init__(self, variant: str = "faithful"):
         self.suffix = {"faithful": "", "strict": "_strict", "omp": "_omp"}[variant]
         self.variant = variant
+        self.isa = "x86-64-v3"
+        # the faithful build closest to the reference Makefile's -march=native:
+        # AVX-512 where the host has it
+        if variant == "faithful" and host_has_avx512() and (REF_DIR / "libref_weno_v4.so").exists():
+            self.suffix, self.isa = "_v4", "x86-64-v4"
         self._weno = None
         self._dg: dict[int, C.CDLL] = {}
 

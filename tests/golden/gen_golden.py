@@ -27,7 +27,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
-from oracle.oracle import Reference  # noqa: E402
+from oracle.oracle import REFERENCE_SOURCES, Reference  # noqa: E402
 from zuikakucfd_b200 import cases  # noqa: E402
 
 STRICT = Reference("strict")
@@ -96,7 +96,7 @@ def gen_weno(store: dict, meta: dict):
 def gen_weno_large(meta: dict, store: dict):
     """The reference's own 2D-Riemann case (256x256) and a 128^2 seeded case:
     hashes of the strict results (bit-exact) plus a few sampled rows."""
-    ref_case = Path("/root/reference/2D-Riemann")
+    ref_case = REFERENCE_SOURCES / "2D-Riemann"
     U, b, da, g = STRICT.weno_load_case(ref_case)
     dt = 0.5 * da / STRICT.weno_max_speed(U, b, da, g)
     store["riemann256/U0"] = U   # the reference's own input case (piecewise constant: compresses to KBs)

@@ -15,7 +15,10 @@
 //     larger grids are rejected with ZK_ERR_ARG before any work is queued;
 //   * the first call on a device looks the array's device address up
 //     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture;
+//     before any stream capture.  The address is cached with the id of the
+//     device's CUDA context; after a context reset (cudaDeviceReset anywhere in
+//     the process) the next call looks it up again, so it too must come before
+//     any stream capture;
 //   * all calls share the one array: calls whose GPU work overlaps (two
 //     streams, two host threads) race.  The status word is cleared by each
 //     call; the stage states and the ghost map are rewritten in full before
@@ -44,7 +47,15 @@ static __device__ __align__(256) unsigned char zk_noalloc_scratch[kScratchBytes]
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-unsigned char* g_addr[kMaxDevices] = {};
+// Per device: the scratch address and the unique id of the CUDA context it
+// was looked up in.  A context reset (cudaDeviceReset by any code in the
+// process) gives the device a new context, possibly with the array at another
+// address; the id tells the cached address apart from a stale one.
+struct ScratchSlot {
+    unsigned char* addr = nullptr;
+    unsigned long long ctx_id = 0;
+};
+ScratchSlot g_slot[kMaxDevices];
 
 // Ghost source map on the device, same rule as the host builder in
 // zk_api.cu (row sweep then column sweep of src_WENO/fluid.cpp:338-370, last
@@ -83,24 +94,65 @@ __global__ void ghost_map_kernel(const int32_t* bct, zk::Grid g, int8_t* kind, i
     }
 }
 
-// Device address of the scratch on the current device (set-up on first use).
+// Unique id of the calling thread's current CUDA context (driver entry
+// points cuCtxGetCurrent / cuCtxGetId, looked up through the runtime so the
+// library needs no link-time libcuda); false when there is none yet or the
+// driver lacks them.
+bool current_context_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(p);
+        p = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(p);
+    });
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+// Device address of the scratch on the current device.  Set-up: the first
+// call on a device (and the first after that device's context was reset)
+// looks the address up with cudaGetSymbolAddress, with the device current;
+// later calls reuse it while the context id is unchanged.
 int scratch_address(unsigned char** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return zk_internal_fail(ZK_ERR_UNSUPPORTED, "device ordinal >= 64");
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, zk_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            char msg[256];
-            snprintf(msg, sizeof msg, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
-            return zk_internal_fail(ZK_ERR_CUDA, msg);
-        }
-        g_addr[dev] = static_cast<unsigned char*>(p);
+    ScratchSlot& slot = g_slot[dev];
+    unsigned long long id = 0;
+    if (slot.addr && current_context_id(&id) && id == slot.ctx_id) {
+        *out = slot.addr;
+        return ZK_OK;
     }
-    *out = g_addr[dev];
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, zk_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e));
+        return zk_internal_fail(ZK_ERR_CUDA, msg);
+    }
+    // the lookup made the device's context current; without an id (old
+    // driver) nothing is cached and every call looks the address up again
+    if (current_context_id(&id)) {
+        slot.addr = static_cast<unsigned char*>(p);
+        slot.ctx_id = id;
+    } else {
+        slot.addr = nullptr;
+    }
+    *out = static_cast<unsigned char*>(p);
     return ZK_OK;
 }
 

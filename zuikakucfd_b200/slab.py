@@ -203,71 +203,3 @@ def slab_step(solvers: Sequence, exchange: Callable[[int], None], dt: float, nst
                 for s in solvers:
                     s.stage_limit(k)
             exchange(k)
-
-
-def _time_workload(method: str, precision: str, order: int, n: int, nslab: int, steps: int = 20) -> dict:
-    """ms per step of one context over an n x n four-quadrant grid (zk_step,
-    CUDA events) and of nslab slabs of it on one GPU (LocalExchange), and ms
-    per step of the exchanges alone."""
-    import torch
-    from . import cases
-    from .fluid import Solver
-
-    def make(b, st):
-        s = Solver(method=method, order=order, precision=precision)
-        s.set_mesh(c.ny, b.shape[1], c.da, c.gamma, b)
-        s.set_state(st)
-        return s
-
-    c = cases.four_quadrant(n, seed=1)
-    U = c.conserved()
-    if method == "dg":
-        st = np.zeros((4, (order + 1) ** 2, c.ny, c.nx))
-        st[:, 0] = U
-        U = st
-        dt = 0.5 * 0.9 / (2.0 * (2 * order + 1)) * cases.cfl_dt(c, 1.0)
-    else:
-        dt = cases.cfl_dt(c, 0.4)
-    w = make(c.bctype, U)
-    w.step(dt, 3)
-    ms_whole = w.step_timed(dt, steps) / steps
-    w.close()
-    solvers = [make(b, s_) for s_, b in split_arrays(U, c.bctype, nslab)]
-    try:
-        ex = LocalExchange(solvers)
-        slab_step(solvers, ex, dt, 3)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(ex.stream)
-        slab_step(solvers, ex, dt, steps)
-        e1.record(ex.stream)
-        e1.synchronize()
-        ms_slab = e0.elapsed_time(e1) / steps
-        e0.record(ex.stream)
-        for _ in range(50):
-            for k in (1, 2, 3):
-                ex(k)
-        e1.record(ex.stream)
-        e1.synchronize()
-        ms_ex = e0.elapsed_time(e1) / 50
-    finally:
-        for s_ in solvers:
-            s_.close()
-    return {"ms_step_whole": ms_whole, f"ms_step_{nslab}slabs_one_gpu": ms_slab, "ms_exchanges_per_step": ms_ex}
-
-
-def main(argv=None) -> int:
-    """Time slabs on one GPU against the whole grid (prints one JSON line)."""
-    import argparse
-    import json
-    ap = argparse.ArgumentParser(description=main.__doc__)
-    ap.add_argument("--slabs", type=int, default=2)
-    a = ap.parse_args(argv)
-    out = {f"{m}_{p}_P{o}_{n}": _time_workload(m, p, o, n, a.slabs)
-           for m, p, o, n in [("weno", "mixed", 2, 2048), ("dg", "mixed", 3, 1024)]}
-    print(json.dumps(out))
-    return 0
-
-
-if __name__ == "__main__":
-    raise SystemExit(main())
