@@ -48,6 +48,13 @@ FLOPS_PER_CELL_STAGE = {("weno", 0): WENO_FLOPS_PER_CELL_STAGE, ("dg", 1): 1700.
                         ("dg", 3): 13200.0}
 
 
+# DRAM bytes per launch of the dominant kernel, from an ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of a small instance of the
+# workload, scaled to a full launch by the updated cells; None where not
+# captured.  Keyed by (workload, precision).
+KERNEL_TRAFFIC: dict = {}
+
+
 def make_workload(name: str, rank: int):
     from zuikakucfd_b200 import cases
     seed = 1000 + rank
@@ -283,53 +290,23 @@ def run_e2e(s, w, U0, args, world, dofs, pg) -> dict:
                     "state H2D from pinned host at start, D2H at end, amortised per step; host wall clock"}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="dg3_fq_2048")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
-    ap.add_argument("--fp64-only", action="store_true", help="time the FP64 path only")
-    ap.add_argument("--batch-policies", default="all,sjf",
-                    help="batch workloads: admission policies to run (the first of 'all' or the list is the value)")
-    args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
-
-    rank, world, local, pg = dist_setup(args.gpus)
-    if args.workload.startswith("slab"):
-        if rank == 0 and args.impl == "ours":
-            print(json.dumps(run_slab(args)), flush=True)
-        if pg is not None:
-            pg.destroy_process_group()
-        return
-    if args.workload.startswith("batch"):
-        if args.impl == "reference":
-            if rank == 0:
-                print(json.dumps(run_reference_batch(args)), flush=True)
-        else:
-            run_batch(args, rank, local, world, pg)
-        if pg is not None:
-            pg.destroy_process_group()
-        return
-    if args.impl == "reference":
-        if rank == 0:
-            print(json.dumps(run_reference_arm(args, make_workload(args.workload, 0))), flush=True)
-        return
-
-    w = make_workload(args.workload, rank)
+def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: bool = True,
+                   cpu_seconds: float = 15.0, refined: bool = True) -> dict | None:
+    """One single-problem workload: the plain FP64 path (the metric's
+    baseline), then the mixed path (the headline), each timed over exactly K
+    steps after W warm-up steps.  rank 0 returns the line's fields, the other
+    ranks None."""
+    w = make_workload(name, rank)
     c = w["case"]
     U0 = c.conserved() if w["method"] == "weno" else c.dg_state(w["order"])
     cells = c.fluid_cells
     dofs = cells * w["dof_per_cell"]
 
-    # plain FP64 path (the baseline of the metric), then the mixed path (the
-    # headline); each timed over exactly K steps after W warm-up steps
+    # fp64: the reference-arithmetic path (--fmad=false, bit-exact against the
+    # reference built without contraction); fp64_fma: the same kernels with
+    # fused multiply-adds (the fastest plain-FP64 path); mixed: the headline
     paths = {}
-    for prec in (["fp64", "mixed"] if not args.fp64_only else ["fp64"]):
+    for prec in (["fp64", "fp64_fma", "mixed"] if not args.fp64_only else ["fp64"]):
         s = open_solver(w, c, U0, prec, local)
         for _ in range(args.warmup):
             s.step(w["dt"], 1)
@@ -344,74 +321,154 @@ def main():
                        "value": world * dofs * args.steps / (ms_max * 1e-3), "solver": s}
     head = "mixed" if "mixed" in paths else "fp64"
     hp = paths[head]
-    # equal-L1 diagnostic: both paths advanced the same steps from the same
-    # state; relative L1 and Linf differences of the cell-average density and
-    # pressure (primitives rho, u, v, p recovered in FP64)
+    # equal-L1 diagnostics: (a) both paths advanced the same steps from the
+    # same state: relative L1 and Linf differences of the cell-average density
+    # and pressure (primitives recovered in FP64); (b) below, each path's L1
+    # error against a 4x finer FP64 solution of the same problem
     eq = None
     if "mixed" in paths:
         q64 = paths["fp64"]["solver"].recover_primitives()
         qmx = paths["mixed"]["solver"].recover_primitives()
         eq = {"steps_compared": args.warmup + args.steps}
-        for name, f in (("density", 0), ("pressure", 3)):
+        for nm, f in (("density", 0), ("pressure", 3)):
             d = np.abs(qmx[f] - q64[f])
-            eq[f"rel_l1_{name}_mixed_vs_fp64"] = float(d.sum() / np.abs(q64[f]).sum())
-            eq[f"rel_linf_{name}_mixed_vs_fp64"] = float(d.max() / np.abs(q64[f]).max())
+            eq[f"rel_l1_{nm}_mixed_vs_fp64"] = float(d.sum() / np.abs(q64[f]).sum())
+            eq[f"rel_linf_{nm}_mixed_vs_fp64"] = float(d.max() / np.abs(q64[f]).max())
 
-    # end to end through the public API with host buffers: the reference
-    # driver's loop (computeMaxSpeed -> dt on the host -> updateMesh), state
-    # uploaded from pinned host memory at the start and read back at the end
-    e2e = None
-    if not args.no_e2e:
-        e2e = run_e2e(hp["solver"], w, U0, args, world, dofs, pg)
-
-    if rank == 0:
-        peaks = measure_peaks(local)
-        peaks_file = ROOT / "MEASURED_PEAKS.json"
-        hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
-        roofs = {}
-        fl = FLOPS_PER_CELL_STAGE[(w["method"], w["order"])]
-        nvar = w["dof_per_cell"]
-        for prec, pth in paths.items():
-            stage_ms = pth["ms"] / (3 * args.steps)  # time of one RK stage (all its launches)
-            achieved = cells * fl / (stage_ms * 1e-3) / 1e12
-            pk = peaks["fp64_tflops"] if prec == "fp64" else peaks["fp32_tflops"]
-            # minimal traffic per stage: stage input + U^n + output (+ kind byte)
-            bpv = 8.0 if (prec == "fp64" or w["method"] == "weno") else 4.0
-            hbm_bytes = cells * (nvar * (bpv + 8.0 + bpv) + 1.0)
-            if w["method"] == "weno":
-                kname = "weno_stage_fp64_kernel" if prec == "fp64" else "weno_stage_mixed_kernel"
-            else:
-                # the mixed P=3 stage runs two threads per cell (dg_mixed.cu kSingleTpc)
-                kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if prec == "fp64"
-                         else "dg_stage_mixed_pair_kernel" if w["order"] == 3 else "dg_stage_mixed_kernel")
-            roofs[prec] = {
-                "bound": "fp64" if prec == "fp64" else "fp32", "achieved": achieved, "peak": pk,
-                "unit": "TFLOP/s", "frac": achieved / pk, "traffic": None,
-                "kernel": kname, "flops_per_cell_stage": fl,
-                "avg_launch_ms": stage_ms,
-                "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU "
-                               "(MEASURED_PEAKS.json has no FP64/FP32 figure)",
-                "hbm": {"achieved_gbs": hbm_bytes / (stage_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
-                        "frac": hbm_bytes / (stage_ms * 1e-3) / 1e9 / hbm_peak}}
-        cpu = {"value": None, "skipped": True} if args.no_cpu_baseline or world > 1 else cpu_baseline(w)
-        out = {"metric": METRIC, "value": hp["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": hp["ms_max"] / args.steps, "higher_is_better": True,
-               "scaling": "weak", "vs_baseline": None,
-               "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
-               "config": {"workload": args.workload, "desc": w["desc"], "grid": [c.ny, c.nx],
-                          "updated_cells": cells, "dof_per_cell": w["dof_per_cell"], "precision": head,
-                          "l2": "working set (3 FP64 states = %.0f MB) larger than the 126 MB L2" %
-                                (3 * U0.nbytes / 1e6),
-                          "parallelism": f"replicas x{world} (independent seeded problems)"},
-               "fp64_value": paths["fp64"]["value"], "equal_l1": eq,
-               "speedup_vs_fp64": hp["value"] / paths["fp64"]["value"],
-               "clocks": hp["clocks"], "e2e": e2e,
-               "gpu_launches": gpu_launches(w, head) * args.steps,
-               "roofline": roofs[head], "roofline_fp64": roofs["fp64"], "cpu_baseline": cpu,
-               "status_word": {p: v["status"] for p, v in paths.items()}, "peaks": peaks}
-        print(json.dumps(out), flush=True)
+    e2e_rec = run_e2e(hp["solver"], w, U0, args, world, dofs, pg) if e2e else None
     for pth in paths.values():
         pth["solver"].close()
+    if rank != 0:
+        return None
+
+    if eq is not None and refined:
+        eq["refined"] = refined_l1(w)
+        pr = eq["refined"]["paths"]
+        base = next(iter(pr))
+        mixed_key = [k for k in pr if k.startswith("mixed")][-1]
+        eq["rel_l1_err_fp64"] = pr[base]["rho_rel_l1_err"]
+        eq["rel_l1_err_mixed"] = pr[mixed_key]["rho_rel_l1_err"]
+        eq["l1_err_ratio_mixed_over_fp64"] = pr[mixed_key]["rho_l1_err_ratio"]
+        eq["equal_l1_met"] = bool(pr[mixed_key]["rho_l1_err_ratio"] <= 1.1)
+    peaks = measure_peaks(local)
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
+    roofs = {}
+    fl = FLOPS_PER_CELL_STAGE[(w["method"], w["order"])]
+    nvar = w["dof_per_cell"]
+    for prec, pth in paths.items():
+        stage_ms = pth["ms"] / (3 * args.steps)  # time of one RK stage (all its launches)
+        achieved = cells * fl / (stage_ms * 1e-3) / 1e12
+        f64 = prec != "mixed"
+        pk = peaks["fp64_tflops"] if f64 else peaks["fp32_tflops"]
+        # minimal traffic per stage: stage input + U^n + output (+ kind byte)
+        bpv = 8.0 if (f64 or w["method"] == "weno") else 4.0
+        hbm_bytes = cells * (nvar * (bpv + 8.0 + bpv) + 1.0)
+        if w["method"] == "weno":
+            kname = "weno_stage_fp64_kernel" if f64 else "weno_stage_mixed_kernel"
+        else:
+            # the mixed P=2, 3 stages run two threads per cell (dg_mixed.cu kSingleTpc)
+            kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if f64
+                     else "dg_stage_mixed_pair_kernel" if w["order"] >= 2 else "dg_stage_mixed_kernel")
+        if prec == "fp64_fma":
+            kname += ", FMA-contracted build"
+        roofs[prec] = {
+            "bound": "fp64" if f64 else "fp32", "achieved": achieved, "peak": pk,
+            "unit": "TFLOP/s", "frac": achieved / pk, "traffic": KERNEL_TRAFFIC.get((name, prec)),
+            "kernel": kname, "flops_per_cell_stage": fl,
+            "avg_launch_ms": stage_ms,
+            "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU "
+                           "(MEASURED_PEAKS.json has no FP64/FP32 figure)",
+            "hbm": {"achieved_gbs": hbm_bytes / (stage_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
+                    "frac": hbm_bytes / (stage_ms * 1e-3) / 1e9 / hbm_peak}}
+    cpu = ({"value": None, "skipped": True} if args.no_cpu_baseline or world > 1
+           else cpu_baseline(w, cpu_seconds))
+    return {"metric": METRIC, "value": hp["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": hp["ms_max"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if head == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": name, "desc": w["desc"], "grid": [c.ny, c.nx],
+                       "updated_cells": cells, "dof_per_cell": w["dof_per_cell"], "precision": head,
+                       "l2": "working set (3 FP64 states = %.0f MB) larger than the 126 MB L2" %
+                             (3 * U0.nbytes / 1e6),
+                       "parallelism": f"replicas x{world} (independent seeded problems)"},
+            "fp64_value": paths["fp64"]["value"], "fp64_fma_value": paths.get("fp64_fma", {}).get("value"),
+            "equal_l1": eq,
+            "speedup_vs_fp64": hp["value"] / paths["fp64"]["value"],
+            "speedup_vs_best_fp64": hp["value"] / max(v["value"] for k, v in paths.items() if k != "mixed"),
+            "clocks": hp["clocks"], "e2e": e2e_rec,
+            "gpu_launches": gpu_launches(w, head) * args.steps,
+            "roofline": roofs[head], "roofline_fp64": roofs["fp64"], "roofline_fp64_fma": roofs.get("fp64_fma"),
+            "cpu_baseline": cpu,
+            "status_word": {p: v["status"] for p, v in paths.items()}, "peaks": peaks}
+
+
+def refined_l1(w: dict) -> dict:
+    """Density L1 error of the workload's FP64 and mixed paths on a 128^2
+    instance of its four-quadrant problem against a 4x finer FP64 solution
+    (512^2) at t = 0.05: the 'at equal L1' of the metric, checked rather than
+    inferred.  DG: FP64 + TVB, mixed + TVB and (P=3) mixed + learned
+    indicator; WENO5: FP64 and mixed."""
+    from zuikakucfd_b200 import accuracy
+    if w["method"] == "dg":
+        P = w["order"]
+        paths = (("fp64", "tvb"), ("mixed", "tvb")) + ((("mixed", "tvb_mlp"),) if P == 3 else ())
+        return accuracy.shock_refined_l1(order=P, n=128, refine=4, t_end=0.05, paths=paths)
+    return accuracy.weno_refined_l1(n=128, refine=4, t_end=0.05)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="dg3_fq_2048")
+    ap.add_argument("--secondary", default="weno_fq_2048,batch64",
+                    help="comma-separated workloads measured after the headline into the line's "
+                         "'secondary' object ('' for none)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-refined", action="store_true", help="skip the refined-solution L1 study")
+    ap.add_argument("--fp64-only", action="store_true", help="time the FP64 path only")
+    ap.add_argument("--batch-policies", default="all,sjf",
+                    help="batch workloads: admission policies to run (the first of 'all' or the list is the value)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    if args.workload.startswith("slab"):
+        if rank == 0 and args.impl == "ours":
+            print(json.dumps(run_slab(args)), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    if args.impl == "reference":
+        if rank == 0:
+            out = (run_reference_batch(args) if args.workload.startswith("batch")
+                   else run_reference_arm(args, make_workload(args.workload, 0)))
+            print(json.dumps(out), flush=True)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    def one(name, primary):
+        if name.startswith("batch"):
+            return run_batch(name, args, rank, local, world, pg,
+                             policies=args.batch_policies if primary else "all",
+                             cpu_seconds=8.0 if primary else 4.0)
+        return measure_single(name, args, rank, world, local, pg, e2e=not args.no_e2e,
+                              cpu_seconds=15.0 if primary else 8.0, refined=not args.no_refined)
+
+    out = one(args.workload, True)
+    sec = [n for n in args.secondary.split(",") if n and n != args.workload]
+    if sec:
+        res = {n: one(n, False) for n in sec}
+        if rank == 0:
+            out["secondary"] = res
+    if rank == 0:
+        print(json.dumps(out), flush=True)
     if pg is not None:
         pg.destroy_process_group()
 
@@ -446,7 +503,8 @@ def batch_cpu_rates(seconds: float = 8.0) -> dict:
     return out
 
 
-def run_batch(args, rank: int, local: int, world: int, pg) -> None:
+def run_batch(name: str, args, rank: int, local: int, world: int, pg, policies: str = "all,sjf",
+              cpu_seconds: float = 8.0) -> dict | None:
     """Batched serving (one step = one SSP-RK3 step of every running problem):
     N seeded four-quadrant problems, sides uniform in {128, ..., 1024}, half
     WENO5 / half DG P=2, mixed precision, each run `steps` steps at its own CFL
@@ -455,7 +513,7 @@ def run_batch(args, rank: int, local: int, world: int, pg) -> None:
     policy "all"); latencies p50/p99 for both admission policies."""
     import torch
     from zuikakucfd_b200.batch import Batch, batch_problems
-    nprob, nsteps = parse_batch(args.workload)
+    nprob, nsteps = parse_batch(name)
     specs = list(batch_problems(nprob, seed=1000 + rank, nsteps=nsteps))
     # pinned host copies of every initial state (the e2e leg uploads from these)
     pinned = [torch.from_numpy(np.ascontiguousarray(s["state"])).pin_memory() for s in specs]
@@ -470,7 +528,7 @@ def run_batch(args, rank: int, local: int, world: int, pg) -> None:
             b.add(**{**s, "nsteps": 3})
         b.run()
     results = {}
-    for policy in args.batch_policies.split(","):
+    for policy in policies.split(","):
         barrier(pg)
         with Batch(policy=policy, graph_steps=10, device=local) as b:
             t0 = time.perf_counter()
@@ -492,14 +550,14 @@ def run_batch(args, rank: int, local: int, world: int, pg) -> None:
     ms = allreduce_max(pg, rep["ms"])
     wall = allreduce_max(pg, head["wall"])
     if rank != 0:
-        return
+        return None
     peaks = measure_peaks(local)
     flops = 3.0 * sum(int((s["bctype"][3:-3, 3:-3] == 0).sum()) * s["nsteps"] *
                       (1330.0 if s["method"] == "weno" else 5300.0) for s in specs)
     achieved = flops / (ms * 1e-3) / 1e12
     cpu = {"value": None, "skipped": True}
     if not args.no_cpu_baseline and world == 1:
-        r = batch_cpu_rates()
+        r = batch_cpu_rates(cpu_seconds)
         if r:
             t_cpu = sum(int((s["bctype"][3:-3, 3:-3] == 0).sum()) * s["nsteps"] *
                         (r["weno"] if s["method"] == "weno" else r["dg2"]) for s in specs)
@@ -515,7 +573,7 @@ def run_batch(args, rank: int, local: int, world: int, pg) -> None:
     out = {"metric": METRIC, "value": world * rep["dof_updates"] / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
            "steps": nsteps, "warmup": 3, "ms_per_step": ms / nsteps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-           "config": {"workload": args.workload, "problems": nprob, "steps_per_problem": nsteps,
+           "config": {"workload": name, "problems": nprob, "steps_per_problem": nsteps,
                       "desc": f"{nprob} seeded four-quadrant problems, sides uniform in {{128..1024 step 128}}, "
                               "first half WENO5 (CFL 0.4), second half DG P=2 (0.5 x dgSafeDt, reference "
                               "limiter), mixed precision, per-problem dt on the device; policy 'all'",
@@ -534,7 +592,7 @@ def run_batch(args, rank: int, local: int, world: int, pg) -> None:
                         "flops": "3 stages x cell-steps x (1330 WENO5, 5300 DG P=2)",
                         "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU"},
            "cpu_baseline": cpu, "peaks": peaks}
-    print(json.dumps(out), flush=True)
+    return out
 
 
 def run_reference_batch(args) -> dict:
@@ -628,19 +686,20 @@ def gpu_launches(w, prec) -> int:
     if w["method"] == "weno":
         return 3
     per_stage = 1 if prec == "mixed" else 3
-    lim = (w["opts"].get(prec, {}) if "fp64" in w["opts"] else w["opts"]).get("limiter", "reference")
+    lim = (w["opts"].get("fp64" if prec == "fp64_fma" else prec, {}) if "fp64" in w["opts"]
+           else w["opts"]).get("limiter", "reference")
     return 3 * (per_stage + (1 if lim in ("tvb", "tvb_mlp") else 0))
 
 
 def open_solver(w, c, U0, precision, device):
     import ctypes as C
     from zuikakucfd_b200 import Solver, _native as N, indicator
-    opts = w["opts"].get(precision, w["opts"]) if "fp64" in w["opts"] else w["opts"]
+    key = "fp64" if precision == "fp64_fma" else precision
+    opts = w["opts"].get(key, w["opts"]) if "fp64" in w["opts"] else w["opts"]
     s = Solver(method=w["method"], order=max(w["order"], 1), precision=precision, device=device, **opts)
     s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
     if opts.get("limiter") == "tvb_mlp":
-        wts = indicator.load()
-        N.check(N.lib().zk_set_indicator(s._h, wts.ctypes.data_as(C.POINTER(C.c_float)), wts.size))
+        s.set_indicator()  # the shipped weights and their calibrated screen
     s.set_state(U0)
     return s
 

@@ -43,8 +43,11 @@ enum {
 enum { ZK_METHOD_WENO = 0, ZK_METHOD_DG = 1 };
 /* FP64: the reference's arithmetic op for op (bit-identical to the reference
  * built with -ffp-contract=off).  MIXED: FP32 reconstruction/fluxes/quadrature
- * with FP64 conserved-state accumulation and FP64 pressure recovery. */
-enum { ZK_PREC_FP64 = 0, ZK_PREC_MIXED = 1 };
+ * with FP64 conserved-state accumulation and FP64 pressure recovery.
+ * FP64_FMA: FP64 throughout with multiply-adds fused, as the reference's own
+ * Makefile build contracts them (within 1e-10 of that build, not bit-identical;
+ * single contexts only, not the batched runner). */
+enum { ZK_PREC_FP64 = 0, ZK_PREC_MIXED = 1, ZK_PREC_FP64_FMA = 2 };
 /* DG limiter: REFERENCE = Persson modal filter + Zhang-Shu positivity
  * (src_DG/fluid.cpp:824-992); NONE; TVB = Cockburn-Shu TVB minmod (M) with
  * characteristic limiting; TVB_MLP = TVB limiting of the cells a learned
@@ -171,19 +174,42 @@ int zk_halo_unpack(zk_ctx* ctx, int stage, int side, const void* dev_buf);
 /* ---- learned troubled-cell indicator (no counterpart in the reference) ----
  * A 40 -> 32 -> 32 -> 32 -> 1 GELU MLP gates the TVB limiter of
  * ZK_LIMITER_TVB_MLP contexts: only cells with a positive logit take the
- * characteristic-limiting branch.  Parameters are the flat FP32 block
- * w1[32][40], b1[32], w2[32][32], b2[32], w3[32][32], b3[32], w4[32], b4
- * (ZK_MLP_NPARAM floats), rounded to BF16 for inference. */
+ * characteristic-limiting branch.  Its inputs for the output of an RK stage
+ * are the cell's rho and E modes in that output and the cell's and its
+ * neighbours' means in the stage's INPUT.  Mixed-precision P=2/3 contexts
+ * evaluate it inside the stage kernel on the tensor cores (BF16) and limit
+ * only the cells it lists; other contexts run a gated pass after each stage.
+ * Parameters are the flat FP32 block w1[32][40], b1[32], w2[32][32], b2[32],
+ * w3[32][32], b3[32], w4[32], b4 (ZK_MLP_NPARAM floats), rounded to BF16 for
+ * inference. */
 #define ZK_MLP_NPARAM 3457
 #define ZK_MLP_IN 40
 int zk_set_indicator(zk_ctx* ctx, const float* params, int nparams);
+/* The indicator's screen: a cell whose 40 features all lie within `screen` of
+ * a constant state's (all 0) is smooth without evaluating the network, and a group of cells evaluated
+ * together (a warp) that is all smooth skips it.  The trained weights come
+ * with a screen calibrated to keep every TVB-troubled training cell; < 0
+ * (the default) evaluates every cell. */
+int zk_set_indicator_screen(zk_ctx* ctx, float screen);
 /* Per cell of the current (FP64) state: the indicator's 40 input features
- * (features[ny*nx][40], may be NULL) and the plain TVB troubled-cell flag
- * (labels[ny][nx], may be NULL).  The state is not modified. */
+ * with the state's own means (features[ny*nx][40], may be NULL) and the plain
+ * TVB troubled-cell flag (labels[ny][nx], may be NULL).  The state is not
+ * modified. */
 int zk_indicator_features(zk_ctx* ctx, float* features, uint8_t* labels);
-/* The indicator's logits[ny*nx] for the current state, computed by the
- * tensor-core inference path the limiter uses (0 for non-updated cells). */
+/* The logits[ny*nx] of the gated pass for the current state with its own
+ * means (0 for non-updated cells). */
 int zk_indicator_logits(zk_ctx* ctx, float* logits);
+/* After zk_stage(ctx, dt, stage): per cell of that stage's output, the
+ * indicator's 40 features (its modes, the stage input's means;
+ * features[ny*nx][40], may be NULL) and the plain TVB flag of the output
+ * (labels[ny][nx], may be NULL) -- the training data of the indicator. */
+int zk_indicator_stage_features(zk_ctx* ctx, int stage, float* features, uint8_t* labels);
+/* zk_stage(ctx, dt, stage) of a mixed-precision DG P=2/3 TVB_MLP context,
+ * returning per cell the features and logit the fused stage kernel computed
+ * (features[ny*nx][40], logits[ny*nx], either may be NULL; 0 for cells not
+ * updated) and the number of cells it listed for limiting (may be NULL). */
+int zk_indicator_stage_logits(zk_ctx* ctx, double dt, int stage, float* features, float* logits,
+                              uint32_t* listed);
 /* Cells the TVB passes limited during the last zk_step (summed over stages). */
 int zk_limited_cells(zk_ctx* ctx, uint32_t* count);
 /* Training on the GPU (hand-written FP32 forward/backward + Adam kernels):

@@ -71,6 +71,29 @@ def forward(p, X):
     return z, (X, z1, h1, z2, h2, z3, h3)
 
 
+def bf16(x):
+    """Round to the nearest BF16 value (ties to even), returned as float32."""
+    a = np.ascontiguousarray(x, np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).reshape(a.shape)
+
+
+def forward_bf16(p, X):
+    """Logits with the arithmetic of the GPU's tensor-core inference: features,
+    every parameter and each hidden layer's GELU output rounded to BF16,
+    products summed in FP32 (here exactly, in float64, then rounded), GELU in
+    FP32 and the output unit in FP32."""
+    W = {k: bf16(v) if np.ndim(v) else bf16(np.float32(v))[()] for k, v in unpack(p).items()}
+    h = bf16(X).astype(np.float64)
+    for l in ("1", "2", "3"):
+        z = (h @ W["w" + l].astype(np.float64).T + W["b" + l]).astype(np.float32)
+        u = np.float32(_K) * (z + np.float32(_C) * z * z * z)
+        g = np.float32(0.5) * z * (np.float32(1.0) + np.tanh(u.astype(np.float64)).astype(np.float32))
+        h = bf16(g).astype(np.float64)
+    return (h @ W["w4"].astype(np.float64) + W["b4"]).astype(np.float32)
+
+
 def loss_and_grad(p, X, y, pos_weight):
     """Mean BCE-with-logits loss (positive weight) and its gradient."""
     W = unpack(p)
@@ -98,38 +121,40 @@ def loss_and_grad(p, X, y, pos_weight):
     return loss, flat
 
 
-def features(P: int, dof: np.ndarray, kind: np.ndarray, src: np.ndarray) -> np.ndarray:
-    """The 40 per-cell features of the GPU indicator (zk_mlp.h) for every cell
-    of a DG state dof[4][NM][ny][nx], neighbours gathered through the ghost
-    map (kind/src as oracle Restatement.ghost_map returns, with slip)."""
+def features(P: int, dof: np.ndarray, kind: np.ndarray, src: np.ndarray, means: np.ndarray | None = None) -> np.ndarray:
+    """The 40 per-cell features of the GPU indicator (zk_mlp.h) for every
+    updated cell: the rho and E modes of the DG state dof[4][NM][ny][nx] and
+    the means (own and neighbours', gathered through the ghost map: kind/src as
+    oracle Restatement.ghost_map returns, with slip) of `means` -- the input
+    of the RK stage whose output dof is -- or of dof itself when None.  FP32
+    arithmetic on FP32-rounded values, as the GPU computes them.  The two
+    scaled means (slots 0 and 16) are centred (minus 1): a constant state's
+    features are all 0."""
     NM = (P + 1) ** 2
     ny, nx = dof.shape[2:]
     out = np.zeros((ny * nx, IN), np.float32)
     flat = dof.reshape(4, NM, -1)
+    mflat = (dof if means is None else means).reshape(4, NM, -1)
 
     def mean(k):
-        s, neg = k, -1
-        if src.flat[k] >= 0:
-            s = int(src.flat[k])
-            neg = 1 if kind.flat[k] == 3 else (2 if kind.flat[k] == 4 else -1)
-        v = flat[:, 0, s].copy()
-        if neg >= 0:
-            v[neg] = -v[neg]
-        return v
+        s = int(src.flat[k]) if src.flat[k] >= 0 else k   # slip walls negate momentum only
+        return np.float32(mflat[0, 0, s]), np.float32(mflat[3, 0, s])
 
     for k in range(ny * nx):
         if kind.flat[k] != 0:
             continue
-        ub = flat[:, 0, k]
-        nb = [mean(k - 1), mean(k + 1), mean(k - nx), mean(k + nx)]
-        sr = np.float32(max(abs(ub[0]), *(abs(v[0]) for v in nb))) + np.float32(1e-12)
-        se = np.float32(max(abs(ub[3]), *(abs(v[3]) for v in nb))) + np.float32(1e-12)
+        ms = [mean(k)] if means is not None else [(np.float32(mflat[0, 0, k]), np.float32(mflat[3, 0, k]))]
+        ms += [mean(k - 1), mean(k + 1), mean(k - nx), mean(k + nx)]
+        sr = np.float32(max(abs(m[0]) for m in ms)) + np.float32(1e-12)
+        se = np.float32(max(abs(m[1]) for m in ms)) + np.float32(1e-12)
         ir, ie = np.float32(1.0) / sr, np.float32(1.0) / se
         for m in range(NM):
             slot = (m // (P + 1)) * 4 + m % (P + 1)
             out[k, slot] = np.float32(flat[0, m, k]) * ir
             out[k, 16 + slot] = np.float32(flat[3, m, k]) * ie
-        for n_, v in enumerate(nb):
-            out[k, 32 + n_] = np.float32(v[0] - ub[0]) * ir
-            out[k, 36 + n_] = np.float32(v[3] - ub[3]) * ie
+        out[k, 0] -= np.float32(1.0)   # the scaled means, centred
+        out[k, 16] -= np.float32(1.0)
+        for n_ in range(4):
+            out[k, 32 + n_] = (ms[1 + n_][0] - ms[0][0]) * ir
+            out[k, 36 + n_] = (ms[1 + n_][1] - ms[0][1]) * ie
     return out

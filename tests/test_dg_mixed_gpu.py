@@ -81,6 +81,24 @@ def test_mixed_equal_l1_against_finer_fp64(P):
     assert emx <= 1.1 * e64, (emx, e64)
 
 
+@pytest.mark.parametrize("P,limiters", [(3, ("tvb", "tvb_mlp")), (2, ("tvb",))])
+def test_tvb_paths_equal_l1_against_finer_fp64(P, limiters):
+    """The metric's path: DG P=3 four-quadrant Riemann problem with TVB
+    limiting (M=50), mixed precision with plain TVB and with the learned
+    indicator gating it, against a 4x finer FP64 + TVB solution (cell averages
+    restricted, same physical time).  Each mixed path's density L1 error is at
+    most 1.1 x the coarse FP64 + TVB path's."""
+    from zuikakucfd_b200 import accuracy
+    paths = (("fp64", "tvb"),) + tuple(("mixed", lim) for lim in limiters)
+    r = accuracy.shock_refined_l1(order=P, n=64, refine=4, t_end=0.05, paths=paths)
+    for key, rec in r["paths"].items():
+        assert rec["status_word"] == 0, (key, rec)
+    e64 = r["paths"]["fp64+tvb"]["rho_l1_err"]
+    for lim in limiters:
+        emx = r["paths"][f"mixed+{lim}"]["rho_l1_err"]
+        assert emx <= 1.1 * e64, (lim, emx, e64, r)
+
+
 def test_mixed_smooth_wave_against_exact():
     """DG P=2 periodic smooth wave at 64^2 to t=0.2: the mixed path's L1 error
     against the exact translated density is within 1.1x the FP64 path's."""

@@ -16,7 +16,7 @@ ERRORS = {1: "ZK_ERR_ARG", 2: "ZK_ERR_STATE", 3: "ZK_ERR_CUDA", 4: "ZK_ERR_NUMER
           5: "ZK_ERR_UNSUPPORTED", 6: "ZK_ERR_IO", 7: "ZK_ERR_TIMEOUT"}
 
 METHOD = {"weno": 0, "dg": 1}
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "fp64_fma": 2}
 LIMITER = {"reference": 0, "none": 1, "tvb": 2, "tvb_mlp": 3}
 FLUX = {"hllc": 0, "hll": 1}
 BOUNDARY = {"exchange": 0, "periodic": 1}
@@ -91,6 +91,10 @@ _SIGS = {
     "zk_indicator_features": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
     "zk_limited_cells": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "zk_indicator_logits": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "zk_set_indicator_screen": (C.c_int, [_P, C.c_float]),
+    "zk_indicator_stage_features": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
+    "zk_indicator_stage_logits": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                            C.POINTER(C.c_uint32)]),
     "zk_mlp_train": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8), C.c_int64,
                                C.POINTER(C.c_float), C.c_int, C.c_int, C.c_float, C.c_float, C.c_uint64,
                                C.POINTER(C.c_float)]),

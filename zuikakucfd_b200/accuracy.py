@@ -81,6 +81,127 @@ def run(n: int = 1024, order: int = 2, t_end: float = 2.0, limiter: str = "tvb",
     return out
 
 
+def restrict(a: np.ndarray, f: int) -> np.ndarray:
+    """Interior (3-cell ring dropped) cell averages of a fine grid restricted
+    to the grid f times coarser."""
+    x = a[3:-3, 3:-3]
+    n0, n1 = x.shape[0] // f, x.shape[1] // f
+    return x.reshape(n0, f, n1, f).mean(axis=(1, 3))
+
+
+def shock_refined_l1(order: int = 3, n: int = 64, refine: int = 4, t_end: float = 0.05, cfl_frac: float = 0.4,
+                     seeds=(2, 3, 5, 7, 8, 9, 10), M: float = 50.0,
+                     paths=(("fp64", "tvb"), ("mixed", "tvb"), ("mixed", "tvb_mlp")), device: int = 0) -> dict:
+    """Density L1 error of DG paths on a seeded four-quadrant Riemann problem
+    against a `refine` times finer FP64 + TVB solution of the same problem at
+    the same physical time (cell averages restricted to the coarse grid).
+
+    The state is the metric's four-quadrant case on the interior [0,1]^2 with
+    the ring outside it (cases.four_quadrant(ring_outside=True)), so both grids
+    hold the same physical problem.  dt = cfl_frac x the reference's DG CFL
+    limit at the coarse grid, shortened so an integer number of steps reaches
+    t_end; the fine run takes refine x the steps at dt / refine.  The first
+    seed whose fine run stays clean (status word 0) is used.  Each coarse path
+    is (precision, limiter); "tvb_mlp" runs the shipped learned indicator.
+    Returns per path the L1 error (mean |rho - rho_fine|) and its ratio to the
+    first path's, plus relative L1 / L-inf differences of each path's density
+    and pressure against the first path."""
+    P = int(order)
+
+    def advance(case, dt, steps, prec, lim):
+        with Solver(method="dg", order=P, precision=prec, limiter=lim, tvb_M=M, device=device) as s:
+            s.set_mesh(case.ny, case.nx, case.da, case.gamma, case.bctype)
+            if lim == "tvb_mlp":
+                s.set_indicator()
+            s.set_state(case.dg_state(P))
+            left = steps
+            while left:
+                k = min(1000, left)
+                s.step(dt, k)
+                left -= k
+            q = s.recover_primitives()
+            return s.get_state(), q, s.status_word()
+
+    t0 = time.perf_counter()
+    for seed in seeds:
+        cc = cases.four_quadrant(n, seed=seed, ring_outside=True)
+        cf = cases.four_quadrant(n * refine, seed=seed, ring_outside=True)
+        lam = cc.da / cases.cfl_dt(cc, 1.0)
+        dt0 = cfl_frac * 0.9 / (2.0 * (2 * P + 1)) * cc.da / lam
+        steps = int(math.ceil(t_end / dt0))
+        dt = t_end / steps
+        fine, _, st = advance(cf, dt / refine, steps * refine, "fp64", "tvb")
+        if st == 0 and np.isfinite(fine[0, 0]).all():
+            break
+    else:
+        raise RuntimeError("no seed gave a clean fine reference run")
+    rho_ref = restrict(fine[0, 0], refine)
+    out = {"order": P, "n": n, "refine": refine, "t_end": t_end, "steps": steps, "dt": dt, "seed": seed,
+           "M": M, "reference": f"FP64 + TVB at {n * refine}^2", "paths": {}}
+    base = None
+    for prec, lim in paths:
+        st, q, sw = advance(cc, dt, steps, prec, lim)
+        rho = st[0, 0, 3:-3, 3:-3]
+        key = f"{prec}+{lim}"
+        rec = {"status_word": sw, "rho_l1_err": float(np.abs(rho - rho_ref).mean()),
+               "rho_rel_l1_err": float(np.abs(rho - rho_ref).sum() / np.abs(rho_ref).sum())}
+        prim = (q[0][3:-3, 3:-3], q[3][3:-3, 3:-3])
+        if base is None:
+            base = (key, rec["rho_l1_err"], prim)
+        else:
+            rec["rho_l1_err_ratio"] = rec["rho_l1_err"] / base[1]
+            for name, a, b in (("density", prim[0], base[2][0]), ("pressure", prim[1], base[2][1])):
+                d = np.abs(a - b)
+                rec[f"rel_l1_{name}_vs_{base[0]}"] = float(d.sum() / np.abs(b).sum())
+                rec[f"rel_linf_{name}_vs_{base[0]}"] = float(d.max() / np.abs(b).max())
+        out["paths"][key] = rec
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
+def weno_refined_l1(n: int = 128, refine: int = 4, t_end: float = 0.05, cfl: float = 0.4, seed: int = 2,
+                    device: int = 0) -> dict:
+    """WENO5 FP64 and mixed paths on a seeded four-quadrant Riemann problem at
+    n^2 against a `refine` times finer FP64 solution at the same physical time
+    (cell averages restricted): density L1 errors, their ratio, and the mixed
+    path's relative L1 / L-inf density and pressure differences from FP64.
+    dt = cfl da / lambda0 (the reference driver's fixed-dt form), shortened so
+    an integer number of steps reaches t_end."""
+    t0 = time.perf_counter()
+    cc = cases.four_quadrant(n, seed=seed, ring_outside=True)
+    cf = cases.four_quadrant(n * refine, seed=seed, ring_outside=True)
+    lam = cc.da / cases.cfl_dt(cc, 1.0)
+    steps = int(math.ceil(t_end * lam / (cfl * cc.da)))
+    dt = t_end / steps
+
+    def advance(case, dt_, steps_, prec):
+        with Solver(method="weno", precision=prec, device=device) as s:
+            s.set_mesh(case.ny, case.nx, case.da, case.gamma, case.bctype)
+            s.set_state(case.conserved())
+            s.step(dt_, steps_)
+            return s.get_state(), s.recover_primitives(), s.status_word()
+
+    fine, _, stf = advance(cf, dt / refine, steps * refine, "fp64")
+    rho_ref = restrict(fine[0], refine)
+    out = {"method": "weno5", "n": n, "refine": refine, "t_end": t_end, "steps": steps, "dt": dt, "seed": seed,
+           "reference": f"FP64 at {n * refine}^2", "reference_status_word": stf, "paths": {}}
+    prims = {}
+    for prec in ("fp64", "mixed"):
+        st, q, sw = advance(cc, dt, steps, prec)
+        rho = st[0, 3:-3, 3:-3]
+        out["paths"][prec] = {"status_word": sw, "rho_l1_err": float(np.abs(rho - rho_ref).mean()),
+                              "rho_rel_l1_err": float(np.abs(rho - rho_ref).sum() / np.abs(rho_ref).sum())}
+        prims[prec] = (q[0][3:-3, 3:-3], q[3][3:-3, 3:-3])
+    mx = out["paths"]["mixed"]
+    mx["rho_l1_err_ratio"] = mx["rho_l1_err"] / out["paths"]["fp64"]["rho_l1_err"]
+    for name, i in (("density", 0), ("pressure", 1)):
+        d = np.abs(prims["mixed"][i] - prims["fp64"][i])
+        mx[f"rel_l1_{name}_vs_fp64"] = float(d.sum() / np.abs(prims["fp64"][i]).sum())
+        mx[f"rel_linf_{name}_vs_fp64"] = float(d.max() / np.abs(prims["fp64"][i]).max())
+    out["seconds"] = time.perf_counter() - t0
+    return out
+
+
 def jet(nx: int = 2048, ny: int = 1024, steps: int = 2000, weno_cfl=(0.003, 0.01, 0.03), dg_cfl=(1.0,),
         precisions=("fp64", "mixed"), device: int = 0) -> dict:
     """The high-Mach jet (cases.high_mach_jet: rho = 5, u = 30 band, gamma =

@@ -31,12 +31,18 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
           f"-I{CSRC}", f"-I{ROOT / 'include'}", "--expt-relaxed-constexpr"]
 STRICT = ["--fmad=false"]
 
-# (source, extra flags)
-SOURCES: list[tuple[str, list[str]]] = [
+# FP64 with fused multiply-add contraction: the same FP64 sources compiled a
+# second time into namespace zk_fma (ZK_PREC_FP64_FMA)
+FMA = ["-DZK_FP64_FMA"]
+
+# (source, extra flags[, object name])
+SOURCES: list[tuple] = [
     ("zk_api.cu", []),
     ("weno_fp64.cu", STRICT),
+    ("weno_fp64.cu", FMA, "weno_fp64_fma.o"),
     ("reduce_fp64.cu", STRICT),
     ("dg_fp64.cu", STRICT),
+    ("dg_fp64.cu", FMA, "dg_fp64_fma.o"),
     ("dg_driver.cu", []),
     ("dg_mixed.cu", ["--use_fast_math"]),
     ("dg_tvb.cu", STRICT),
@@ -67,8 +73,8 @@ def _stale(obj: Path, src: Path, deps: list[Path]) -> bool:
     return any(p.stat().st_mtime > t for p in [src, *deps, Path(__file__)])
 
 
-def _compile(src: Path, flags: list[str], force: bool, verbose: bool) -> Path:
-    obj = OBJ / (src.stem + ".o")
+def _compile(src: Path, flags: list[str], force: bool, verbose: bool, obj_name: str | None = None) -> Path:
+    obj = OBJ / (obj_name or src.stem + ".o")
     if not force and not _stale(obj, src, _headers()):
         return obj
     cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(src), "-o", str(obj)]
@@ -87,7 +93,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(parents=True, exist_ok=True)
     LIB.parent.mkdir(parents=True, exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda sf: _compile(CSRC / sf[0], sf[1], force, verbose), SOURCES))
+        objs = list(ex.map(lambda sf: _compile(CSRC / sf[0], sf[1], force, verbose, *sf[2:]), SOURCES))
     if force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), *map(str, objs)]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -58,4 +58,18 @@ struct DGArgs {
     int want_lam;        // 1: report the max corner wave speed of the fluid cells written
 };
 
+// The learned indicator fused into a mixed-precision stage: fragment-packed
+// weights (MlpFrag, mlp_infer.cuh), the list the flagged cells are appended
+// to (pitched indices, capacity cap), its device counter, and an optional
+// per-cell debug output (features and logit, 41 floats per pitched cell),
+// and the screen of smooth cells.
+struct FusedIndicator {
+    const void* mlp;
+    int32_t* list;
+    uint32_t* count;
+    uint32_t cap;
+    float* dbg;
+    float screen;  // cells within this of a constant state's features skip the network (< 0: none)
+};
+
 }  // namespace zk

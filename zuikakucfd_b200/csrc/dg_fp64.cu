@@ -24,7 +24,17 @@
 #include "dg_common.cuh"
 #include "zk_internal.h"
 
-namespace zk {
+// Built twice: with --fmad=false as the reference-arithmetic path (namespace
+// zk), and with -DZK_FP64_FMA, fused multiply-adds contracted, as the
+// ZK_PREC_FP64_FMA path (namespace zk_fma).
+#ifdef ZK_FP64_FMA
+#define ZK_FP64_NS zk_fma
+#else
+#define ZK_FP64_NS zk
+#endif
+
+namespace ZK_FP64_NS {
+using namespace zk;
 
 __constant__ DGTab c_dgtab[3];
 
@@ -714,4 +724,4 @@ cudaError_t launch_dg_limit_fp64(int P, const DGArgs& a, cudaStream_t s) {
     }
 }
 
-}  // namespace zk
+}  // namespace ZK_FP64_NS

@@ -21,6 +21,7 @@
 
 #include "batch.cuh"
 #include "dg_common.cuh"
+#include "mlp_infer.cuh"
 #include "zk_internal.h"
 
 namespace zk {
@@ -67,6 +68,14 @@ struct MixArgs {
     uint32_t* status;
     const double* phic;  // basis at the 4 cell corners [NM][4] (LAM kernels only)
     double gamma64;      // gamma in FP64 (LAM kernels only)
+    // learned troubled-cell indicator fused into the stage (MLP kernels only):
+    // weights, the list the flagged cells are appended to, its count and capacity
+    const MlpFrag* mlp;
+    int32_t* list;
+    uint32_t* count;
+    uint32_t cap;
+    float* dbg;  // non-null: per updated cell k, dbg[k*41 ..] = the 40 features and the logit
+    float screen;  // cells whose features deviate from a constant state's by <= screen skip the network
 };
 
 __device__ __forceinline__ float fmaxr(float a, float b) { return (a < b) ? b : a; }
@@ -741,6 +750,113 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     return umax;
 }
 
+// Shared memory of the fused indicator: one [16][MLP_TILE_KP] BF16 feature
+// tile per warp (8 warps).  It reuses the interface-flux region, free once
+// every cell has taken its face integrals, where that region is large enough
+// (P = 3), else it follows the stage's own shared memory.  The weights are
+// read through L1 (staging them in shared memory left L1 too small for the
+// stage: measured slower).
+constexpr size_t kMlpTileBytes = 8 * 16 * MLP_TILE_KP * sizeof(uint16_t);
+__host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
+template <int P, int MTY>
+constexpr bool mlp_tiles_in_flux() {
+    return sizeof(float) * (P + 1) * 4 * (MTY * (MTX + 1) + (MTY + 1) * MTX) >= kMlpTileBytes;
+}
+
+// Round-to-nearest BF16 pair, lo in the low half.
+__device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// The learned indicator fused into the two-threads-per-cell stage (every
+// thread of the CTA calls it, once, after the cell phase).  Features
+// (zk_mlp.h) of the cell a lane pair just wrote: half 0 the rho modes, half 1
+// the E modes (FP32 values of the combine, acc[h]), scaled by the largest
+// |mean| of the cell and its four neighbours in the stage INPUT (the tile's
+// shared memory, ghosts already filled), and the neighbour-mean differences of
+// that input.  Screen: a cell whose features all lie within `screen` of a
+// constant state's (all 0) is smooth; a warp
+// whose 16 cells are all smooth skips the network.  Otherwise the warp's 16
+// cells go through the MLP on the tensor cores (mlp_logits16), and half 0 of
+// every updated, unscreened cell with a positive logit appends the cell to the
+// list, which the TVB list pass then limits.
+template <int P>
+__device__ __forceinline__ void indicator_epilogue(const MixArgs& a, const float* sd, uint16_t* ftiles, int slot,
+                                                   int h, bool upd, const float (&acc)[2][(P + 1) * (P + 1)],
+                                                   size_t k) {
+    constexpr int NQ = P + 1, NM = NQ * NQ, VP = vpitch(NM);
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, row = lane >> 1;
+    float f[20];
+#pragma unroll
+    for (int i = 0; i < 20; ++i) f[i] = 0.0f;
+    float dev = 0.0f;  // largest |feature| of this half: the deviation from a constant state
+    if (upd) {
+        const int var = h ? 3 : 0;
+        const float m0 = sd[slot * VP + var * NM];
+        const float mL = sd[(slot - 1) * VP + var * NM], mR = sd[(slot + 1) * VP + var * NM];
+        const float mU = sd[(slot - SX) * VP + var * NM], mD = sd[(slot + SX) * VP + var * NM];
+        const float sc = fmaxf(fmaxf(fmaxf(fabsf(m0), fabsf(mL)), fmaxf(fabsf(mR), fabsf(mU))), fabsf(mD)) + 1e-12f;
+        const float is = 1.0f / sc;
+#pragma unroll
+        for (int px = 0; px < NQ; ++px)
+#pragma unroll
+            for (int py = 0; py < NQ; ++py) f[px * 4 + py] = (h ? acc[1][px * NQ + py] : acc[0][px * NQ + py]) * is;
+        f[0] = __fsub_rn(f[0], 1.0f);
+        f[16] = (mL - m0) * is;
+        f[17] = (mR - m0) * is;
+        f[18] = (mU - m0) * is;
+        f[19] = (mD - m0) * is;
+#pragma unroll
+        for (int i = 0; i < 20; ++i) dev = fmaxf(dev, fabsf(f[i]));
+    }
+    dev = fmaxf(dev, __shfl_xor_sync(FULL, dev, 1));
+    const bool cand = upd && !(dev <= a.screen);
+    __syncthreads();  // every face integral is taken: the flux region may hold the feature tiles
+    const bool warp_runs = __any_sync(FULL, cand);
+    float z = -INFINITY;
+    if (warp_runs) {
+        uint16_t* tile = ftiles + (threadIdx.x >> 5) * 16 * MLP_TILE_KP;
+        uint32_t* trow = reinterpret_cast<uint32_t*>(tile + row * MLP_TILE_KP);
+        // row layout (words of BF16 pairs): rho modes 0..7, E modes 8..15, rho
+        // differences 16..17, E differences 18..19, zero padding 20..23
+#pragma unroll
+        for (int w = 0; w < 8; ++w) trow[8 * h + w] = bf16x2(f[2 * w], f[2 * w + 1]);
+        trow[16 + 2 * h] = bf16x2(f[16], f[17]);
+        trow[17 + 2 * h] = bf16x2(f[18], f[19]);
+        trow[20 + 2 * h] = 0u;
+        trow[21 + 2 * h] = 0u;
+        __syncwarp();
+        float lo, hi;
+        mlp_logits16(a.mlp, tile, lane, lo, hi);
+        const int src = 4 * (row & 7);
+        const float zl = __shfl_sync(FULL, lo, src), zh = __shfl_sync(FULL, hi, src);
+        if (cand) z = row < 8 ? zl : zh;
+    }
+    if (a.dbg && upd) {
+        float* o = a.dbg + k * 41;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) o[16 * h + i] = f[i];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) o[32 + 4 * h + i] = f[16 + i];
+        if (h == 0) o[40] = z;
+    }
+    const bool app = h == 0 && z > 0.0f;
+    const unsigned m = __ballot_sync(FULL, app);
+    if (m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(a.count, (uint32_t)__popc(m));
+        base = __shfl_sync(FULL, base, leader);
+        if (app) {
+            const uint32_t idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+            if (idx < a.cap) a.list[idx] = (int32_t)k;
+        }
+    }
+}
+
 // Own half (two variables, 2 NM floats, contiguous in a cell-major slot) as
 // vectors of VW floats.
 template <int NM>
@@ -782,7 +898,7 @@ __device__ __forceinline__ void join_pair(int h, float a0, float a1, float o0, f
 // bits.  Shuffles run under masks taken by ballot over lanes that are all
 // present: the face loop has a warp-uniform trip count and the cell phase
 // returns only after its last shuffle.
-template <int P, typename TIn, typename TOut, int MTY, bool LAM = false>
+template <int P, typename TIn, typename TOut, int MTY, bool LAM = false, bool MLP = false>
 __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int i0, float* smem) {
     constexpr int MNT = MTX * MTY, NT = 2 * MNT, SY = MTY + 2;
     constexpr int NQ = P + 1, NM = NQ * NQ;
@@ -942,6 +1058,9 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         }
     }
     __syncthreads();  // every interface flux is in shared memory
+    // the cell phase of lanes whose cell is in the grid; the fused indicator
+    // after it is entered by every lane of the warp
+    const auto cell_phase = [&]() -> double {
     if (!inside) return 0.0;
     if (kd == KIND_UPDATED) {
         // face integrals of this half's variables (order of stage_tile)
@@ -1201,6 +1320,17 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     }
     if (flags) atomicOr(a.status, flags);
     return umax;
+    };
+    const double umax_cell = cell_phase();
+    if constexpr (MLP) {
+        // feature tiles: the flux region, or after the stage's shared memory
+        constexpr size_t own = sizeof(float) * (VP * SD + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SD;
+        uint16_t* tiles = mlp_tiles_in_flux<P, MTY>() ? reinterpret_cast<uint16_t*>(sfx)
+                                                     : reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(smem) +
+                                                                                   align16(own));
+        if (a.stage > 0) indicator_epilogue<P>(a, sd, tiles, slot, h, inside && kd == KIND_UPDATED, acc, k);
+    }
+    return umax_cell;
 }
 
 template <int P, int MTY>
@@ -1226,14 +1356,21 @@ constexpr int pair_thread_budget(int P) { return P == 1 ? 1024 : P == 3 ? 512 : 
 // CTAs of 128 threads, the same 16 warps per SM) ran 9% slower at P = 3 (the
 // 1-cell halo is 2.1x the tile's cells instead of 1.6x).
 constexpr int kPairRows = 4;
-template <int P>
-constexpr int pair_min_blocks() {
-    return batch_min_blocks(MTX * 2 * kPairRows, pair_thread_budget(P), smem_bytes<P, kPairRows>());
+// Shared memory of the single-problem pair kernel, with the indicator's
+// feature tiles when MLP.
+template <int P, bool MLP>
+constexpr size_t pair_smem_bytes() {
+    return MLP && !mlp_tiles_in_flux<P, kPairRows>() ? align16(smem_bytes<P, kPairRows>()) + kMlpTileBytes
+                                                    : smem_bytes<P, kPairRows>();
 }
-template <int P, typename TIn, typename TOut>
-__global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P>()) dg_stage_mixed_pair_kernel(MixArgs a) {
+template <int P, bool MLP = false>
+constexpr int pair_min_blocks() {
+    return batch_min_blocks(MTX * 2 * kPairRows, pair_thread_budget(P), pair_smem_bytes<P, MLP>());
+}
+template <int P, typename TIn, typename TOut, bool MLP>
+__global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P, MLP>()) dg_stage_mixed_pair_kernel(MixArgs a) {
     extern __shared__ __align__(16) float smem[];
-    stage_tile_pair<P, TIn, TOut, kPairRows>(a, blockIdx.x * MTX, blockIdx.y * kPairRows, smem);
+    stage_tile_pair<P, TIn, TOut, kPairRows, false, MLP>(a, blockIdx.x * MTX, blockIdx.y * kPairRows, smem);
 }
 
 // Threads per cell of the single-problem stage kernel, per P (measured at
@@ -1334,12 +1471,13 @@ cudaError_t batch_p(int variant, int stage, const DgItem* items, const int* dir,
     }
 }
 
-template <int P, typename TIn, typename TOut>
+template <int P, typename TIn, typename TOut, bool MLP>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
     constexpr bool pair = kSingleTpc[P] == 2;
+    static_assert(pair || !MLP, "the fused indicator runs in the two-threads-per-cell kernel");
     constexpr int rows = pair ? kPairRows : 4;
-    constexpr size_t sm = smem_bytes<P, rows>();
-    auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut> : dg_stage_mixed_kernel<P, TIn, TOut>;
+    constexpr size_t sm = pair ? pair_smem_bytes<P, MLP>() : smem_bytes<P, rows>();
+    auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut, MLP> : dg_stage_mixed_kernel<P, TIn, TOut>;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1353,12 +1491,19 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int P, typename TIn, typename TOut>
+cudaError_t launch_io(const MixArgs& a, cudaStream_t s) {
+    if constexpr (kSingleTpc[P] == 2)
+        if (a.mlp) return launch_one<P, TIn, TOut, true>(a, s);
+    return launch_one<P, TIn, TOut, false>(a, s);
+}
+
 template <int P>
 cudaError_t launch_p(const MixArgs& a, int in_fp64, int out_fp64, cudaStream_t s) {
-    if (in_fp64 && !out_fp64) return launch_one<P, double, float>(a, s);
-    if (!in_fp64 && !out_fp64) return launch_one<P, float, float>(a, s);
-    if (!in_fp64 && out_fp64) return launch_one<P, float, double>(a, s);
-    return launch_one<P, double, double>(a, s);
+    if (in_fp64 && !out_fp64) return launch_io<P, double, float>(a, s);
+    if (!in_fp64 && !out_fp64) return launch_io<P, float, float>(a, s);
+    if (!in_fp64 && out_fp64) return launch_io<P, float, double>(a, s);
+    return launch_io<P, double, double>(a, s);
 }
 
 }  // namespace
@@ -1430,12 +1575,27 @@ int dg_mixed_batch_tiles(int variant, int ny, int nx) {
 
 // One mixed-precision DG stage: cur (double if in_fp64 else float) -> out
 // (double if out_fp64 else float).
+
+// Whether the single-problem stage of order P can run the fused indicator.
+bool dg_mixed_fuses_indicator(int P) { return P >= 1 && P <= 3 && kSingleTpc[P] == 2; }
+// With `ind` (P = 2, 3: the two-threads-per-cell kernels) the learned
+// indicator runs fused in the stage and appends the cells it flags to
+// ind->list; the caller then runs the TVB list pass.
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
-                                  cudaStream_t s) {
+                                  const FusedIndicator* ind, cudaStream_t s) {
     MixArgs a{cur, un, out, kind, gsrc, g, dt, (float)(0.5 / da), (float)gamma, stage, limiter, hll, (float)s0,
               status};
+    if (ind) {
+        if (kSingleTpc[P < 1 || P > 3 ? 0 : P] != 2) return cudaErrorInvalidValue;
+        a.mlp = static_cast<const MlpFrag*>(ind->mlp);
+        a.list = ind->list;
+        a.count = ind->count;
+        a.cap = ind->cap;
+        a.dbg = ind->dbg;
+        a.screen = ind->screen;
+    }
     switch (P) {
         case 1: return launch_p<1>(a, in_fp64, out_fp64, s);
         case 2: return launch_p<2>(a, in_fp64, out_fp64, s);

@@ -9,6 +9,11 @@
 // means are never modified, so the sweep is race-free in place.  Compiled with
 // --fmad=false: the FP64 instantiation is bit-identical to the oracle's C
 // restatement (oracle/dg_oracle.c: limit_tvb_all).
+//
+// The indicator's features (zk_mlp.h) take the cell's modes from the stage
+// output and the means from the stage INPUT, the same values the fused
+// mixed-precision stage kernel has in its tile (dg_mixed.cu).  List mode
+// (tvb_list_kernel) limits only the cells the fused indicator listed.
 #include <cuda_bf16.h>
 
 #include "dg_common.cuh"
@@ -118,7 +123,25 @@ struct TvbArgs {
     float* features;   // features mode: [ncell][40] output, no limiting
     uint32_t* nflag;   // count of limited cells, may be null
     float* logits;     // with mlp: per-cell logit output [ny*nx], no limiting
+    const void* means; // stage input whose means feed the features (null: the state itself)
+    int means_fp64;    // means is double (else float)
+    const int32_t* list;    // list mode: pitched cell indices to limit ...
+    const uint32_t* count;  // ... and their number
+    float screen;      // gated: cells within this of a constant state's features are smooth (< 0: none)
 };
+
+__device__ __forceinline__ float load_mean(const void* p, int fp64, size_t i) {
+    return fp64 ? (float)static_cast<const double*>(p)[i] : static_cast<const float*>(p)[i];
+}
+
+// Mean of (rho, E) of the cell at k of the features' means source, through
+// the fill map (a slip wall negates only momentum, so rho and E copy).
+__device__ __forceinline__ void nb_mean_re(const TvbArgs& a, size_t k, size_t vs, float& rho, float& E) {
+    const int8_t kd = a.kind[k] & KIND_MASK;
+    const size_t s = kd >= KIND_COPY ? (size_t)a.gsrc[k] : k;
+    rho = load_mean(a.means, a.means_fp64, s);
+    E = load_mean(a.means, a.means_fp64, 3 * vs + s);
+}
 
 // ---- indicator inference on the tensor cores --------------------------------------
 // One warp evaluates the MLP for its 32 cells with mma.sync m16n8k16 BF16
@@ -272,6 +295,9 @@ constexpr int kTvbRows = 1;  // rows per CTA
 
 template <typename T, int P>
 __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gated, int i, int j);
+template <typename T, int P>
+__device__ __forceinline__ void tvb_limit(const TvbArgs& a, size_t k, const T (&ub)[4], const T (&uL)[4],
+                                          const T (&uR)[4], const T (&uU)[4], const T (&uD)[4]);
 
 // 6 CTAs per SM (80 registers, some spilled): the pass is latency-bound, and
 // the extra resident warps beat the 4 CTAs that 110 registers allowed (+1.9%
@@ -313,11 +339,26 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
 #pragma unroll
         for (int s = 0; s < MLP_IN; ++s) f[s] = 0.0f;
         if (active) {
-            // rho and E modes, slot px*4+py, scaled by the largest |mean| around
-            const float sr = (float)tmax_(tmax_(tmax_(fabs(ub[0]), fabs(uL[0])), tmax_(fabs(uR[0]), fabs(uU[0]))),
-                                          fabs(uD[0])) + 1e-12f;
-            const float se = (float)tmax_(tmax_(tmax_(fabs(ub[3]), fabs(uL[3])), tmax_(fabs(uR[3]), fabs(uU[3]))),
-                                          fabs(uD[3])) + 1e-12f;
+            // means of the stage input (own, L, R, U, D) for rho and E
+            float mr[5], me[5];
+            if (a.means) {
+                const size_t ks[5] = {k, k - 1, k + 1, k - (size_t)a.g.pitch, k + (size_t)a.g.pitch};
+#pragma unroll
+                for (int n = 0; n < 5; ++n) nb_mean_re(a, ks[n], vs, mr[n], me[n]);
+            } else {
+                const T* src[5] = {ub, uL, uR, uU, uD};
+#pragma unroll
+                for (int n = 0; n < 5; ++n) {
+                    mr[n] = (float)src[n][0];
+                    me[n] = (float)src[n][3];
+                }
+            }
+            // rho and E modes of the output, slot px*4+py, scaled by the
+            // largest |mean| around; neighbour-mean differences
+            const float sr = fmaxf(fmaxf(fmaxf(fabsf(mr[0]), fabsf(mr[1])), fmaxf(fabsf(mr[2]), fabsf(mr[3]))),
+                                   fabsf(mr[4])) + 1e-12f;
+            const float se = fmaxf(fmaxf(fmaxf(fabsf(me[0]), fabsf(me[1])), fmaxf(fabsf(me[2]), fabsf(me[3]))),
+                                   fabsf(me[4])) + 1e-12f;
             const float ir = 1.0f / sr, ie = 1.0f / se;
 #pragma unroll
             for (int m = 0; m < NM; ++m) {
@@ -325,11 +366,12 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
                 f[slot] = (float)d[(size_t)m * plane + k] * ir;
                 f[16 + slot] = (float)d[3 * vs + (size_t)m * plane + k] * ie;
             }
-            const T* nb[4] = {uL, uR, uU, uD};
+            f[0] -= 1.0f;  // the scaled means, centred: a constant state's features are 0
+            f[16] -= 1.0f;
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
-                f[32 + n] = (float)(nb[n][0] - ub[0]) * ir;
-                f[36 + n] = (float)(nb[n][3] - ub[3]) * ie;
+                f[32 + n] = (mr[1 + n] - mr[0]) * ir;
+                f[36 + n] = (me[1 + n] - me[0]) * ie;
             }
         }
         if (a.features) {
@@ -339,7 +381,18 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
                 for (int s = 0; s < MLP_IN; ++s) a.features[cell * MLP_IN + s] = f[s];
             }
         } else {
-            const float z = mlp_logit_mma(S, threadIdx.x >> 5, threadIdx.x & 31, f);
+            // the screen of the fused indicator (dg_mixed.cu): features within
+            // `screen` of a constant state's are smooth; a warp of smooth cells
+            // skips the network
+            float dev = 0.0f;
+#pragma unroll
+            for (int s = 0; s < MLP_IN; ++s) dev = fmaxf(dev, fabsf(f[s]));
+            const bool cand = active && !(dev <= a.screen);
+            float z = -INFINITY;
+            if (__any_sync(0xffffffffu, cand)) {
+                const float zz = mlp_logit_mma(S, threadIdx.x >> 5, threadIdx.x & 31, f);
+                if (cand) z = zz;
+            }
             if (a.logits) {
                 if (active) a.logits[(size_t)i * a.g.nx + j] = z;
                 return;
@@ -348,6 +401,17 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
         }
     }
     if (!active) return;
+    tvb_limit<T, P>(a, k, ub, uL, uR, uU, uD);
+}
+
+// The TVB test of one updated cell (own mean ub, neighbour means) and, when
+// it fires, the characteristic limiting of its modes in place.
+template <typename T, int P>
+__device__ __forceinline__ void tvb_limit(const TvbArgs& a, size_t k, const T (&ub)[4], const T (&uL)[4],
+                                          const T (&uR)[4], const T (&uU)[4], const T (&uD)[4]) {
+    constexpr int NM = (P + 1) * (P + 1);
+    const size_t plane = a.g.plane, vs = (size_t)NM * plane;
+    T* d = static_cast<T*>(a.state);
     const T mh2 = T(a.M) * T(a.da) * T(a.da);
     T ax[4], ay[4], dxp[4], dxm[4], dyp[4], dym[4], lx[4], ly[4];
 #pragma unroll
@@ -375,6 +439,40 @@ __device__ __forceinline__ void tvb_cell(const TvbArgs& a, MlpSmem& S, bool gate
     }
 }
 
+// List mode: the cells the fused indicator of the mixed stage kernel flagged
+// (pitched indices list[0 .. *count)), each through tvb_limit on the stage
+// output; a grid-stride loop over the device-side count.
+template <typename T, int P>
+__global__ void __launch_bounds__(128) tvb_list_kernel(TvbArgs a) {
+    constexpr int NM = (P + 1) * (P + 1);
+    const size_t vs = (size_t)NM * a.g.plane;
+    const T* d = static_cast<const T*>(a.state);
+    const uint32_t n = *a.count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const size_t k = (size_t)a.list[t];
+        if (a.flags) a.flags[k] = 0;
+        T ub[4], uL[4], uR[4], uU[4], uD[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ub[c] = d[(size_t)c * vs + k];
+        nb_mean<T>(d, a.kind, a.gsrc, k - 1, vs, uL);
+        nb_mean<T>(d, a.kind, a.gsrc, k + 1, vs, uR);
+        nb_mean<T>(d, a.kind, a.gsrc, k - (size_t)a.g.pitch, vs, uU);
+        nb_mean<T>(d, a.kind, a.gsrc, k + (size_t)a.g.pitch, vs, uD);
+        tvb_limit<T, P>(a, k, ub, uL, uR, uU, uD);
+    }
+}
+
+template <typename T>
+cudaError_t launch_list_t(int P, const TvbArgs& a, int grid, cudaStream_t s) {
+    switch (P) {
+        case 1: tvb_list_kernel<T, 1><<<grid, 128, 0, s>>>(a); break;
+        case 2: tvb_list_kernel<T, 2><<<grid, 128, 0, s>>>(a); break;
+        case 3: tvb_list_kernel<T, 3><<<grid, 128, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_t(int P, const TvbArgs& a, cudaStream_t s) {
     dim3 grid((a.g.nx + 127) / 128, (a.g.ny + kTvbRows - 1) / kTvbRows);
@@ -391,9 +489,20 @@ cudaError_t launch_t(int P, const TvbArgs& a, cudaStream_t s) {
 
 cudaError_t launch_dg_tvb(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
                           double da, double gamma, double M, uint8_t* flags, const MlpPacked* mlp,
-                          float* features, uint32_t* nflag, float* logits, cudaStream_t s) {
-    TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, mlp, features, nflag, logits};
+                          float* features, uint32_t* nflag, float* logits, const void* means, bool means_fp64,
+                          float screen, cudaStream_t s) {
+    TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, mlp, features, nflag, logits, means, means_fp64 ? 1 : 0,
+              nullptr, nullptr, screen};
     return fp64 ? launch_t<double>(P, a, s) : launch_t<float>(P, a, s);
+}
+
+// TVB limiting of the listed cells only (list mode), `grid` CTAs of 128 threads.
+cudaError_t launch_dg_tvb_list(int P, void* state, bool fp64, const int8_t* kind, const int32_t* gsrc, const Grid& g,
+                               double da, double gamma, double M, uint8_t* flags, uint32_t* nflag,
+                               const int32_t* list, const uint32_t* count, int grid, cudaStream_t s) {
+    TvbArgs a{state, kind, gsrc, g, da, gamma, M, flags, nullptr, nullptr, nflag, nullptr, nullptr, 0, list, count,
+              -1.0f};
+    return fp64 ? launch_list_t<double>(P, a, grid, s) : launch_list_t<float>(P, a, grid, s);
 }
 
 }  // namespace zk

@@ -16,7 +16,17 @@
 #include "zk_common.cuh"
 #include "zk_kernels.h"
 
-namespace zk {
+// Built twice: with --fmad=false as the reference-arithmetic path (namespace
+// zk), and with -DZK_FP64_FMA, fused multiply-adds contracted, as the
+// ZK_PREC_FP64_FMA path (namespace zk_fma).
+#ifdef ZK_FP64_FMA
+#define ZK_FP64_NS zk_fma
+#else
+#define ZK_FP64_NS zk
+#endif
+
+namespace ZK_FP64_NS {
+using namespace zk;
 namespace {
 
 // A tile is 32 x TY cells; NW warps (TY + 1 by default) take the 2 TY + 2
@@ -336,4 +346,4 @@ cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double*
     return cudaGetLastError();
 }
 
-}  // namespace zk
+}  // namespace ZK_FP64_NS

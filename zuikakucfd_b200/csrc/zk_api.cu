@@ -139,7 +139,7 @@ int zk_create(const zk_options* opt, zk_ctx** out) {
         return fail(ZK_ERR_ARG, "unknown method %d", opt->method);
     if (opt->method == ZK_METHOD_DG && (opt->order < 1 || opt->order > 3))
         return fail(ZK_ERR_ARG, "DG order must be 1..3, got %d", opt->order);
-    if (opt->precision != ZK_PREC_FP64 && opt->precision != ZK_PREC_MIXED)
+    if (opt->precision != ZK_PREC_FP64 && opt->precision != ZK_PREC_MIXED && opt->precision != ZK_PREC_FP64_FMA)
         return fail(ZK_ERR_ARG, "unknown precision %d", opt->precision);
     if (opt->limiter < ZK_LIMITER_REFERENCE || opt->limiter > ZK_LIMITER_TVB_MLP)
         return fail(ZK_ERR_ARG, "unknown limiter %d", opt->limiter);
@@ -335,9 +335,9 @@ int zk_status_word(zk_ctx* c, uint32_t* out) {
 // One SSP-RK3 step of the WENO path on the device state (enqueue only).
 static int weno_step_fp64(zk_ctx* c, double dt) {
     const double dtdx = dt / c->da, dtdy = dt / c->da;
-    ZK_CUDA(launch_weno_stage_fp64(c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 1, c->d_status, c->stream));
-    ZK_CUDA(launch_weno_stage_fp64(c->S1, c->Un, c->S2, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 2, c->d_status, c->stream));
-    ZK_CUDA(launch_weno_stage_fp64(c->S2, c->Un, c->Un, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 3, c->d_status, c->stream));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 1, c->d_status, c->stream));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S1, c->Un, c->S2, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 2, c->d_status, c->stream));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S2, c->Un, c->Un, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 3, c->d_status, c->stream));
     return ZK_OK;
 }
 
@@ -444,7 +444,7 @@ int zk_rhs(zk_ctx* c, double dt, double* host_dU) {
         if (int rc = zk_dg_rhs(c, c->S1)) return rc;
     } else {
         const double dtdx = dt / c->da, dtdy = dt / c->da;
-        ZK_CUDA(launch_weno_stage_fp64(c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 0, c->d_status, c->stream));
+        ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 0, c->d_status, c->stream));
     }
     ZK_CUDA(cudaMemcpy2DAsync(host_dU, sizeof(double) * c->g.nx, c->S1, sizeof(double) * c->g.pitch,
                               sizeof(double) * c->g.nx, (size_t)c->nvar * c->g.ny,

@@ -12,6 +12,7 @@
 
 struct zk_ctx {
     zk_options opt{};
+    bool fma() const { return opt.precision == ZK_PREC_FP64_FMA; }
     zk::Grid g{};
     double da = 0.0, gamma = 0.0;
     int nm = 1;    // modes per variable (1 for WENO)
@@ -36,8 +37,12 @@ struct zk_ctx {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void* dg = nullptr;  // DG driver state
-    void* mlp = nullptr;          // device MlpWeights (learned indicator), BF16-rounded
+    void* mlp = nullptr;          // device MlpPacked (learned indicator, separate gated pass), BF16-rounded
+    void* mlp_frag = nullptr;     // device MlpFrag (the same weights for the indicator fused in the stage)
     bool mlp_set = false;
+    float mlp_screen = -1.0f;     // indicator screen (zk_set_indicator_screen); < 0: every cell evaluated
+    int32_t* d_list = nullptr;    // cells the fused indicator flagged in the current stage (pitched indices)
+    uint32_t* d_lcount = nullptr; // their counts, one per RK stage, cleared at each step's stage 1
     uint8_t* d_flags = nullptr;   // TVB troubled-cell flags of the last pass, pitched
     uint32_t* d_nflag = nullptr;  // cells the TVB passes limited during the last zk_step
 
@@ -58,7 +63,7 @@ void zk_dg_release(zk_ctx* c);
 int zk_dg_step(zk_ctx* c, double dt);
 int zk_dg_rhs(zk_ctx* c, double* dU_dev);
 int zk_dg_limit(zk_ctx* c);
-int zk_dg_after_stage(zk_ctx* c, void* state, bool fp64);
+int zk_dg_after_stage(zk_ctx* c, int stage);
 int zk_dg_stage(zk_ctx* c, double dt, int stage);
 int zk_dg_stage_limit(zk_ctx* c, int stage);
 

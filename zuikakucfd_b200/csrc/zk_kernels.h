@@ -13,6 +13,28 @@ cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double*
                                    double dtdx, double dtdy, double gamma, int stage,
                                    uint32_t* status, cudaStream_t s);
 
+}  // namespace zk
+
+namespace zk_fma {
+// The FP64 WENO stage compiled with fused multiply-add contraction
+// (ZK_PREC_FP64_FMA); same arguments as zk::launch_weno_stage_fp64.
+cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
+                                   const int8_t* kind, const int32_t* gsrc, const zk::Grid& g,
+                                   double dtdx, double dtdy, double gamma, int stage,
+                                   uint32_t* status, cudaStream_t s);
+}  // namespace zk_fma
+
+namespace zk {
+
+// The FP64 WENO stage of a context's precision: the reference-arithmetic
+// kernel, or (fma) the contracted one.
+inline cudaError_t launch_weno_stage_f64(bool fma, const double* Ucur, const double* Un, double* Uout,
+                                         const int8_t* kind, const int32_t* gsrc, const Grid& g, double dtdx,
+                                         double dtdy, double gamma, int stage, uint32_t* status, cudaStream_t s) {
+    return fma ? zk_fma::launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s)
+               : launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s);
+}
+
 cudaError_t launch_fill_ghosts(double* U, const int8_t* kind, const int32_t* gsrc, const Grid& g,
                                int nvar, int nm, int sms, cudaStream_t s);
 cudaError_t launch_max_speed_weno(const double* U, const Grid& g, double gamma,

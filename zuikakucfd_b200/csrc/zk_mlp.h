@@ -1,11 +1,15 @@
 // The learned troubled-cell indicator: a 40 -> 32 -> 32 -> 32 -> 1 MLP with
-// GELU activations.  Inputs (per cell, from the FP64/FP32 DG state):
-//   f[0..15]   rho modes, slot px*4+py, divided by s_rho = max |rho mean| over
-//              the cell and its 4 neighbours
-//   f[16..31]  E modes, same slots, divided by s_E
+// GELU activations.  Inputs per cell of an RK stage's output (FP32 values of
+// the FP64/FP32 DG states), the "means" being those of the stage's INPUT:
+//   f[0..15]   the output's rho modes, slot px*4+py, divided by s_rho = max
+//              |rho mean| over the cell and its 4 neighbours, minus 1 in slot
+//              0 (the mean), so that a constant state's features are all 0
+//   f[16..31]  the output's E modes, same slots, divided by s_E (slot 16 - 1)
 //   f[32..35]  (rho mean of neighbour L, R, U, D - own rho mean) / s_rho
 //   f[36..39]  the same for E
-// Output: a logit; > 0 flags the cell for TVB characteristic limiting.
+// Output: a logit; > 0 flags the cell for TVB characteristic limiting.  The
+// means of the stage input are in the mixed-precision stage kernel's tile, so
+// the indicator runs inside that kernel (dg_mixed.cu, mlp_infer.cuh).
 #pragma once
 
 #include <cuda_runtime.h>

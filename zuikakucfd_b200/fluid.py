@@ -127,6 +127,18 @@ class Solver:
         N.check(N.lib().zk_recover_primitives(self._h, N.dptr(out)))
         return out
 
+    def set_indicator(self, params=None, screen: float | None = None) -> None:
+        """Weights of the learned troubled-cell indicator (limiter "tvb_mlp"):
+        a flat FP32 block of MLP_NPARAM values; None loads the trained weights
+        shipped with the package together with their calibrated screen
+        (zk_set_indicator_screen).  `screen` overrides it (< 0: none)."""
+        from . import indicator
+        w = np.ascontiguousarray(indicator.load() if params is None else params, np.float32)
+        N.check(N.lib().zk_set_indicator(self._h, w.ctypes.data_as(C.POINTER(C.c_float)), w.size))
+        if screen is None:
+            screen = indicator.load_screen() if params is None else -1.0
+        N.check(N.lib().zk_set_indicator_screen(self._h, float(screen)))
+
     def status_word(self) -> int:
         v = C.c_uint32()
         N.check(N.lib().zk_status_word(self._h, C.byref(v)))

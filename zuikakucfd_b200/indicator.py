@@ -4,8 +4,11 @@ A 40 -> 32 -> 32 -> 32 -> 1 GELU MLP (the layout is documented in
 include/zuikaku.h) trained on labels the plain TVB-minmod indicator produces
 on seeded four-quadrant runs, then used by DG contexts with
 limiter="tvb_mlp": only the cells it flags take the characteristic-limiting
-branch.  Training runs on the GPU through the library's own forward/backward/
-Adam kernels (zk_mlp_train); nothing here runs on the CPU but data plumbing.
+branch.  Its inputs for an RK stage's output are the output's rho and E modes
+and the means of the stage's input, which the mixed-precision stage kernel
+holds in its tile, so the indicator runs inside that kernel.  Training runs
+on the GPU through the library's own forward/backward/Adam kernels
+(zk_mlp_train); nothing here runs on the CPU but data plumbing.
 
     python -m zuikakucfd_b200.indicator train --out weights.npz
     python -m zuikakucfd_b200.indicator eval --weights weights.npz
@@ -52,15 +55,29 @@ def features_and_labels(solver) -> tuple[np.ndarray, np.ndarray]:
     return X, y
 
 
+def stage_features_and_labels(solver, stage: int) -> tuple[np.ndarray, np.ndarray]:
+    """(features[ny*nx][40], TVB labels[ny*nx]) of the output of RK stage
+    `stage`, which solver.stage(dt, stage) has just computed: the output's
+    modes with the stage input's means, labelled by the plain TVB indicator
+    on the output."""
+    n = solver.ny * solver.nx
+    X = np.zeros((n, NIN), np.float32)
+    y = np.zeros(n, np.uint8)
+    N.check(N.lib().zk_indicator_stage_features(solver._h, int(stage), _fp(X), y.ctypes.data_as(C.POINTER(C.c_uint8))))
+    return X, y
+
+
 def generate_dataset(n_runs: int = 64, n: int = 512, order: int = 3, steps: int = 160, snapshots: int = 4,
                      per_run: int = 160_000, seed0: int = 5000, M: float = 50.0, device: int = 0,
                      cfl_frac: float = 0.5, verbose: bool = True):
     """Seeded four-quadrant runs advanced with the plain TVB limiter; at
-    `snapshots` times the state is advanced one unlimited step and every
-    updated cell's features are labelled by the TVB indicator.  Per run all
-    troubled cells are kept and the rest is filled with randomly chosen
-    smooth cells up to `per_run` samples.  Runs whose state goes non-finite
-    are dropped.  Returns X[N][40], y[N], metadata."""
+    `snapshots` times the state is advanced one unlimited FP64 step, stage by
+    stage, and every updated cell of each stage's output is a sample: its
+    features (the output's modes, the stage input's means) labelled by the
+    TVB indicator on the output.  Per run all troubled cells are kept and the
+    rest is filled with randomly chosen smooth cells up to `per_run` samples.
+    Runs whose state goes non-finite are dropped.  Returns X[N][40], y[N],
+    metadata."""
     from .fluid import Solver
     rng = np.random.default_rng(seed0)
     Xs, ys, used = [], [], []
@@ -88,11 +105,11 @@ def generate_dataset(n_runs: int = 64, n: int = 512, order: int = 3, steps: int 
                     ok = False
                     break
                 raw.set_state(st)
-                raw.step(dt, 1)
-                X, y = features_and_labels(raw)
-                X, y = X[upd], y[upd]
-                rx.append(X)
-                ry.append(y)
+                for stage in (1, 2, 3):
+                    raw.stage(dt, stage)
+                    X, y = stage_features_and_labels(raw, stage)
+                    rx.append(X[upd])
+                    ry.append(y[upd])
             if not ok or not rx:
                 continue
             X = np.concatenate(rx)
@@ -109,7 +126,8 @@ def generate_dataset(n_runs: int = 64, n: int = 512, order: int = 3, steps: int 
     X = np.concatenate(Xs)
     y = np.concatenate(ys)
     meta = {"runs": len(used), "seeds": used, "grid": n, "order": order, "steps": steps, "snapshots": snapshots,
-            "M": M, "samples": int(len(y)), "positives": int(y.sum())}
+            "M": M, "samples": int(len(y)), "positives": int(y.sum()), "features": "stage output modes, stage input means",
+            "seconds": time.time() - t0}
     return X, y, meta
 
 
@@ -136,15 +154,44 @@ def logits(params: np.ndarray, X: np.ndarray, bf16: bool = True, device: int = 0
     return out
 
 
-def agreement(params: np.ndarray, X: np.ndarray, y: np.ndarray, bf16: bool = True, device: int = 0) -> dict:
+def deviation(X: np.ndarray) -> np.ndarray:
+    """Largest |feature| of each row, its deviation from a constant state's
+    (all features 0): the screen's quantity."""
+    return np.abs(X).max(axis=1)
+
+
+def calibrate_screen(X: np.ndarray, y: np.ndarray, margin: float = 0.5) -> dict:
+    """The screen: `margin` x the smallest deviation of any TVB-troubled
+    training cell, so that no troubled training cell is screened out."""
+    d = deviation(X)
+    pos = y.astype(bool)
+    tau = float(margin * d[pos].min()) if pos.any() else -1.0
+    return {"screen": tau, "pos_dev_min": float(d[pos].min()) if pos.any() else None,
+            "pos_dev_q1e-4": float(np.quantile(d[pos], 1e-4)) if pos.any() else None,
+            "neg_screened": float((d[~pos] <= tau).mean()) if (~pos).any() else None}
+
+
+def agreement(params: np.ndarray, X: np.ndarray, y: np.ndarray, bf16: bool = True, device: int = 0,
+              screen: float = -1.0) -> dict:
     """Flag agreement with the TVB labels: accuracy, missed-discontinuity rate
-    (TVB-troubled cells the network does not flag), false-flag rate."""
+    (TVB-troubled cells the indicator does not flag), false-flag rate.  With a
+    screen (>= 0) the indicator flags a cell when its deviation exceeds the
+    screen and the network's logit is positive."""
     f = logits(params, X, bf16, device) > 0
+    if screen >= 0:
+        f &= deviation(X) > screen
     t = y.astype(bool)
     tp = int((f & t).sum())
     return {"accuracy": float((f == t).mean()), "missed_rate": float(((~f) & t).sum() / max(1, t.sum())),
             "false_flag_rate": float((f & ~t).sum() / max(1, (~t).sum())),
             "precision": float(tp / max(1, f.sum())), "flag_rate": float(f.mean()), "n": int(len(y))}
+
+
+def load_screen(path=None) -> float:
+    """The screen calibrated with the weights (-1 when they carry none)."""
+    z = np.load(path or DEFAULT_WEIGHTS)
+    meta = json.loads(str(z["meta"])) if "meta" in z.files else {}
+    return float(meta.get("screen", -1.0))
 
 
 def save(path, params, meta: dict | None = None) -> None:
@@ -164,6 +211,8 @@ def main(argv=None) -> int:
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--out", required=True)
+    t.add_argument("--recalibrate", default=None,
+                   help="keep the weights of this file and only calibrate the screen on fresh data")
     t.add_argument("--runs", type=int, default=64)
     t.add_argument("--grid", type=int, default=512)
     t.add_argument("--per-run", type=int, default=160_000)
@@ -174,15 +223,35 @@ def main(argv=None) -> int:
     e.add_argument("--runs", type=int, default=4)
     e.add_argument("--grid", type=int, default=512)
     a = ap.parse_args(argv)
+    if a.cmd == "train" and a.recalibrate:
+        p = load(a.recalibrate)
+        old = json.loads(str(np.load(a.recalibrate)["meta"]))
+        X, y, _ = generate_dataset(n_runs=a.runs, n=a.grid, per_run=a.per_run)
+        old.update(calibrate_screen(X, y))
+        Xh, yh, _ = generate_dataset(n_runs=a.holdout_runs, n=a.grid, per_run=a.per_run, seed0=9000)
+        old["holdout_with_screen"] = agreement(p, Xh, yh, screen=old["screen"])
+        old["holdout_screened"] = float((deviation(Xh) <= old["screen"]).mean())
+        save(a.out, p, old)
+        print(json.dumps({k: old[k] for k in ("screen", "pos_dev_min", "pos_dev_q1e-4", "neg_screened",
+                                               "holdout_with_screen", "holdout_screened")}), flush=True)
+        return 0
     if a.cmd == "train":
         X, y, meta = generate_dataset(n_runs=a.runs, n=a.grid, per_run=a.per_run)
         print(json.dumps({k: v for k, v in meta.items() if k != "seeds"}), flush=True)
+        t0 = time.time()
         p, losses = train(X, y, epochs=a.epochs)
+        meta["train_seconds"] = time.time() - t0
+        meta.update(calibrate_screen(X, y))
         Xh, yh, mh = generate_dataset(n_runs=a.holdout_runs, n=a.grid, per_run=a.per_run, seed0=9000)
         ag = agreement(p, Xh, yh)
-        meta.update({"epoch_loss": losses.tolist(), "holdout": ag, "holdout_seeds": mh["seeds"]})
+        ags = agreement(p, Xh, yh, screen=meta["screen"])
+        meta.update({"epoch_loss": losses.tolist(), "holdout": ag, "holdout_with_screen": ags,
+                     "holdout_screened": float((deviation(Xh) <= meta["screen"]).mean()),
+                     "holdout_seeds": mh["seeds"]})
         save(a.out, p, meta)
-        print(json.dumps({"epoch_loss": losses.tolist(), "holdout": ag}), flush=True)
+        print(json.dumps({k: meta[k] for k in ("epoch_loss", "holdout", "holdout_with_screen", "screen",
+                                                "pos_dev_min", "pos_dev_q1e-4", "neg_screened",
+                                                "holdout_screened")}), flush=True)
     else:
         p = load(a.weights)
         Xh, yh, _ = generate_dataset(n_runs=a.runs, n=a.grid, seed0=9000)
