@@ -58,6 +58,12 @@ enum { ZK_FLUX_HLLC = 0, ZK_FLUX_HLL = 1 };
  * reference at one rank); PERIODIC refills them with their periodic image
  * inside the 3-wide ring before every RHS evaluation. */
 enum { ZK_BOUNDARY_EXCHANGE = 0, ZK_BOUNDARY_PERIODIC = 1 };
+/* WENO face reconstruction: WENO5 (the reference's scheme,
+ * src_WENO/fluid.cpp:230-263) or MUSCL with the slope limiter of the
+ * reference's muscl_reconstruct (src_WENO/fluid.cpp:203-225, which its solver
+ * never calls): minmod, van Leer, superbee.  MUSCL runs at FP64 and FP64_FMA
+ * precision on single contexts. */
+enum { ZK_RECON_WENO5 = 0, ZK_RECON_MUSCL_MINMOD = 1, ZK_RECON_MUSCL_VANLEER = 2, ZK_RECON_MUSCL_SUPERBEE = 3 };
 
 typedef struct zk_options {
     int method;     /* ZK_METHOD_*                           */
@@ -68,12 +74,13 @@ typedef struct zk_options {
     int boundary;   /* ZK_BOUNDARY_*                         */
     int device;     /* CUDA device ordinal                   */
     double tvb_M;   /* TVB constant M (default 50)           */
+    int recon;      /* ZK_RECON_* (WENO only; default WENO5) */
 } zk_options;
 
 typedef struct zk_ctx zk_ctx;
 
 /* Fills *opt with defaults: WENO, P=2, FP64, reference limiter, HLLC,
- * exchange boundary, device 0, M=50. */
+ * exchange boundary, device 0, M=50, WENO5 reconstruction. */
 void zk_default_options(zk_options* opt);
 
 int zk_create(const zk_options* opt, zk_ctx** out);
@@ -222,6 +229,15 @@ int zk_mlp_grad(int device, const float* X, const uint8_t* y, int64_t n, const f
                 float* grad, float* loss);
 /* Logits of n samples (bf16 != 0: BF16-rounded weights, as in inference). */
 int zk_mlp_forward(int device, const float* X, int64_t n, const float* params, int bf16, float* logits);
+
+/* Failure-detection self-test (no counterpart in the reference): runs stage 1
+ * of a mixed-precision WENO context with its TMA barrier expecting 16 bytes
+ * more than the copy delivers and its bounded wait limited to spin_limit polls
+ * (0: 1), so every CTA's wait runs out; each CTA records STATUS_TIMEOUT (8) in
+ * the status word, settles the missing bytes, waits for its copy to land and
+ * leaves without writing.  *status_out receives the status word; the state is
+ * untouched and the context stays usable.  No GPU fault is involved. */
+int zk_selftest_tma_timeout(zk_ctx* ctx, uint32_t spin_limit, uint32_t* status_out);
 
 /* FMA-throughput microbenchmark of one device: kind 0 = FP64, 1 = FP32;
  * writes the achieved dense TFLOP/s (2 flops per FMA).  Roofline denominator

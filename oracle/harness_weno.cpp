@@ -203,4 +203,12 @@ void refw_hllc(const double* UL, const double* UR, double gamma, double* F) {
     hllcFlux(UL[0], UL[1], UL[2], UL[3], UR[0], UR[1], UR[2], UR[3], gamma, F[0], F[1], F[2], F[3]);
 }
 
+// muscl_reconstruct (src_WENO/fluid.cpp:203-225) over n stencils s[n][4] =
+// (UL2, UL1, UR1, UR2) with limiter 0 (minmod), 1 (van Leer), 2 (superbee):
+// out[n][2] = (UL, UR).
+void refw_muscl(const double* s, int n, int limiter, double* out) {
+    for (int i = 0; i < n; ++i)
+        muscl_reconstruct(s[4 * i], s[4 * i + 1], s[4 * i + 2], s[4 * i + 3], limiter, out[2 * i], out[2 * i + 1]);
+}
+
 }  // extern "C"

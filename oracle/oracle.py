@@ -79,6 +79,9 @@ class Restatement:
         L = C.CDLL(str(RESTATEMENT))
         L.ow_rhs.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double, C.c_int, _D]
         L.ow_step.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double, C.c_int, C.c_int]
+        L.ow_step_recon.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double, C.c_int, C.c_int,
+                                    C.c_int]
+        L.ow_muscl.argtypes = [C.c_double] * 4 + [C.c_int, _D, _D]
         L.ow_max_speed.argtypes = [C.c_int, C.c_int, C.c_double, _D]
         L.ow_max_speed.restype = C.c_double
         L.ow_recover.argtypes = [C.c_int, C.c_int, C.c_double, _D, _D]
@@ -113,12 +116,25 @@ class Restatement:
         self.L.ow_rhs(ny, nx, da, gamma, _d(U), _i(b), dt, int(periodic), _d(dU))
         return U, dU
 
-    def weno_step(self, U, bct, da, gamma, dt, nsteps=1, periodic=False):
+    def weno_step(self, U, bct, da, gamma, dt, nsteps=1, periodic=False, recon=0):
+        """recon 0: WENO5 (the reference path); 1..3: MUSCL with minmod, van
+        Leer, superbee (the reference's muscl_reconstruct as the face
+        reconstruction)."""
         U = np.array(U, dtype=np.float64, order="C")
         b = np.ascontiguousarray(bct, dtype=np.int32)
         ny, nx = b.shape
-        self.L.ow_step(ny, nx, da, gamma, _d(U), _i(b), dt, int(nsteps), int(periodic))
+        self.L.ow_step_recon(ny, nx, da, gamma, _d(U), _i(b), dt, int(nsteps), int(periodic), int(recon))
         return U
+
+    def muscl(self, stencils, limiter):
+        """ow_muscl over stencils[n][4] = (UL2, UL1, UR1, UR2): out[n][2] = (UL, UR)."""
+        st = np.ascontiguousarray(stencils, np.float64)
+        out = np.empty((len(st), 2))
+        ul, ur = C.c_double(), C.c_double()
+        for i, (a, b, c, d) in enumerate(st):
+            self.L.ow_muscl(a, b, c, d, int(limiter), C.byref(ul), C.byref(ur))
+            out[i] = ul.value, ur.value
+        return out
 
     def weno_max_speed(self, U, gamma):
         U = np.ascontiguousarray(U, dtype=np.float64)
@@ -249,6 +265,7 @@ class Reference:
             L.refw_max_speed.restype = C.c_double
             L.refw_recover.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, _D]
             L.refw_hllc.argtypes = [_D, _D, C.c_double, _D]
+            L.refw_muscl.argtypes = [_D, C.c_int, C.c_int, _D]
             L.refw_case_info.argtypes = [C.c_char_p, _I, _I, _D, _D]
             L.refw_load_case.argtypes = [C.c_char_p, _D, _I]
             L.refw_step_slabs_timed.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _D, _I, C.c_double,
@@ -332,6 +349,13 @@ class Reference:
         F = np.empty(4)
         self._w().refw_hllc(_d(L), _d(R), gamma, _d(F))
         return F
+
+    def muscl(self, stencils, limiter):
+        """The reference's muscl_reconstruct over stencils[n][4]: out[n][2] = (UL, UR)."""
+        st = np.ascontiguousarray(stencils, np.float64)
+        out = np.empty((len(st), 2))
+        self._w().refw_muscl(_d(st), len(st), int(limiter), _d(out))
+        return out
 
     def weno_load_case(self, folder):
         ny, nx = C.c_int(), C.c_int()

@@ -8,6 +8,7 @@
  * --fmad=false.  The parity tests pin it against the reference build.
  *
  * Layout: U[4][ny][nx] row-major (row = y, row 0 on top), bct int32[ny][nx]. */
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 #include "oracle_common.h"
@@ -42,6 +43,40 @@ void ow_weno5(double UL2, double UL1, double UP, double UR1, double UR2, double 
     double e0 = 0.1 / (s0 * s0), e1 = 0.6 / (s1 * s1), e2 = 0.3 / (s2 * s2);
     double inv2 = 1.0 / (e0 + e1 + e2);
     *ur = (e0 * qR0 + e1 * qR1 + e2 * qR2) * inv2;
+}
+
+/* muscl_reconstruct, src_WENO/fluid.cpp:203-225 (dead code in the reference,
+ * kept there as an option): cells UL2, UL1 | UR1, UR2 around the face; slopes
+ * from the one-sided differences through minmod (limiter 0), van Leer (1) or
+ * superbee (2); returns the left and right face states. */
+static double ow_minmod2(double a, double b) { return a * b <= 0.0 ? 0.0 : (fabs(a) < fabs(b) ? a : b); }
+static double ow_vanleer(double a, double b) {
+    double ab = a * b;
+    return ab <= 0.0 ? 0.0 : 2.0 * ab / (a + b);
+}
+static double ow_superbee(double a, double b) {
+    double s1 = ow_minmod2(a, 2.0 * b), s2 = ow_minmod2(2.0 * a, b);
+    return s1 * s2 <= 0.0 ? 0.0 : (fabs(s1) > fabs(s2) ? s1 : s2);
+}
+void ow_muscl(double UL2, double UL1, double UR1, double UR2, int limiter, double* ul, double* ur) {
+    double dL = UL1 - UL2, dC = UR1 - UL1, dR = UR2 - UR1;
+    double sL = 0.0, sR = 0.0;
+    switch (limiter) {
+        case 0: sL = ow_minmod2(dL, dC); sR = ow_minmod2(dC, dR); break;
+        case 1: sL = ow_vanleer(dL, dC); sR = ow_vanleer(dC, dR); break;
+        case 2: sL = ow_superbee(dL, dC); sR = ow_superbee(dC, dR); break;
+        default: break;
+    }
+    *ul = UL1 + 0.5 * sL;
+    *ur = UR1 - 0.5 * sR;
+}
+
+/* Face states of the face between cells a1 and b1 of the stencil
+ * a3 a2 a1 | b1 b2 b3: WENO5 (recon 0) or MUSCL with limiter recon - 1. */
+static void ow_face(int recon, double a3, double a2, double a1, double b1, double b2, double b3, double* ul,
+                    double* ur) {
+    if (recon == 0) ow_weno5(a3, a2, a1, b1, b2, b3, ul, ur);
+    else ow_muscl(a2, a1, b1, b2, recon - 1, ul, ur);
 }
 
 /* hllcFlux (WENO variant), src_WENO/fluid.cpp:268-317: x-direction HLLC with
@@ -96,7 +131,7 @@ static void apply_fill(int nfield, size_t plane, const signed char* kind, const 
 
 /* Flux difference of one fluid cell, src_WENO/fluid.cpp:402-460 (dU includes dt). */
 static void cell_rhs(int nx, size_t plane, const double* U, size_t k, double gamma, double dtdx,
-                     double dtdy, double out[4]) {
+                     double dtdy, int recon, double out[4]) {
     double s[13][4];
     /* stencil order: P, r1 r2 r3, l1 l2 l3, u1 u2 u3 (row-1..), d1 d2 d3 (row+1..) */
     const long off[13] = {0, 1, 2, 3, -1, -2, -3, -(long)nx, -2L * nx, -3L * nx, nx, 2L * nx, 3L * nx};
@@ -104,10 +139,10 @@ static void cell_rhs(int nx, size_t plane, const double* U, size_t k, double gam
         for (int c = 0; c < 4; ++c) s[n][c] = U[c * plane + (size_t)((long)k + off[n])];
     double QLr[4], QRr[4], QLl[4], QRl[4], QLd[4], QRd[4], QLu[4], QRu[4];
     for (int c = 0; c < 4; ++c) {
-        ow_weno5(s[5][c], s[4][c], s[0][c], s[1][c], s[2][c], s[3][c], &QLr[c], &QRr[c]);
-        ow_weno5(s[6][c], s[5][c], s[4][c], s[0][c], s[1][c], s[2][c], &QLl[c], &QRl[c]);
-        ow_weno5(s[8][c], s[7][c], s[0][c], s[10][c], s[11][c], s[12][c], &QLd[c], &QRd[c]);
-        ow_weno5(s[9][c], s[8][c], s[7][c], s[0][c], s[10][c], s[11][c], &QLu[c], &QRu[c]);
+        ow_face(recon, s[5][c], s[4][c], s[0][c], s[1][c], s[2][c], s[3][c], &QLr[c], &QRr[c]);
+        ow_face(recon, s[6][c], s[5][c], s[4][c], s[0][c], s[1][c], s[2][c], &QLl[c], &QRl[c]);
+        ow_face(recon, s[8][c], s[7][c], s[0][c], s[10][c], s[11][c], s[12][c], &QLd[c], &QRd[c]);
+        ow_face(recon, s[9][c], s[8][c], s[7][c], s[0][c], s[10][c], s[11][c], &QLu[c], &QRu[c]);
     }
     double Fr[4], Fl[4], Fd[4], Fu[4];
     ow_hllc(QLr, QRr, gamma, Fr);
@@ -139,7 +174,7 @@ static ow_map map_new(int ny, int nx, const int* bct, int periodic) {
 }
 static void map_free(ow_map* m) { free(m->kind); free(m->src); }
 
-static void rhs_with_map(const ow_map* m, double da, double gamma, double* U, double dt, double* dU) {
+static void rhs_with_map(const ow_map* m, double da, double gamma, double* U, double dt, int recon, double* dU) {
     const int ny = m->ny, nx = m->nx;
     const size_t plane = (size_t)ny * nx;
     apply_fill(4, plane, m->kind, m->src, U);
@@ -148,7 +183,7 @@ static void rhs_with_map(const ow_map* m, double da, double gamma, double* U, do
     for (size_t k = 0; k < plane; ++k) {
         if (m->kind[k] != ZK_CELL_UPDATED) continue;
         double o[4];
-        cell_rhs(nx, plane, U, k, gamma, dtdx, dtdy, o);
+        cell_rhs(nx, plane, U, k, gamma, dtdx, dtdy, recon, o);
         for (int c = 0; c < 4; ++c) dU[c * plane + k] = o[c];
     }
 }
@@ -157,24 +192,32 @@ static void rhs_with_map(const ow_map* m, double da, double gamma, double* U, do
 void ow_rhs(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
             int periodic, double* dU) {
     ow_map m = map_new(ny, nx, bct, periodic);
-    rhs_with_map(&m, da, gamma, U, dt, dU);
+    rhs_with_map(&m, da, gamma, U, dt, 0, dU);
     map_free(&m);
 }
 
 /* updateMesh, src_WENO/fluid.cpp:468-493: Shu-Osher SSP-RK3 on whole arrays. */
+/* updateMesh with the face reconstruction `recon` (0: WENO5, 1..3: MUSCL with
+ * minmod, van Leer, superbee). */
+void ow_step_recon(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
+                   int nsteps, int periodic, int recon);
 void ow_step(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
              int nsteps, int periodic) {
+    ow_step_recon(ny, nx, da, gamma, U, bct, dt, nsteps, periodic, 0);
+}
+void ow_step_recon(int ny, int nx, double da, double gamma, double* U, const int* bct, double dt,
+                   int nsteps, int periodic, int recon) {
     const size_t n = (size_t)4 * ny * nx;
     ow_map m = map_new(ny, nx, bct, periodic);
     double* Un = (double*)malloc(sizeof(double) * n);
     double* dU = (double*)malloc(sizeof(double) * n);
     for (int s = 0; s < nsteps; ++s) {
         memcpy(Un, U, sizeof(double) * n);
-        rhs_with_map(&m, da, gamma, U, dt, dU);
+        rhs_with_map(&m, da, gamma, U, dt, recon, dU);
         for (size_t k = 0; k < n; ++k) U[k] = Un[k] + dU[k];
-        rhs_with_map(&m, da, gamma, U, dt, dU);
+        rhs_with_map(&m, da, gamma, U, dt, recon, dU);
         for (size_t k = 0; k < n; ++k) U[k] = 0.75 * Un[k] + 0.25 * (U[k] + dU[k]);
-        rhs_with_map(&m, da, gamma, U, dt, dU);
+        rhs_with_map(&m, da, gamma, U, dt, recon, dU);
         for (size_t k = 0; k < n; ++k) U[k] = (1.0 / 3.0) * Un[k] + (2.0 / 3.0) * (U[k] + dU[k]);
     }
     free(Un); free(dU);

@@ -207,6 +207,25 @@ def gen_points(store: dict, meta: dict):
     store["points/phi2_pts"] = pts
 
 
+def gen_muscl(store: dict, meta: dict):
+    """The reference's muscl_reconstruct (src_WENO/fluid.cpp:203-225) on
+    seeded stencils (UL2, UL1, UR1, UR2) with sign changes, equal neighbours,
+    zeros and opposite slopes, for limiters 0 (minmod), 1 (van Leer), 2
+    (superbee), strict and Makefile-faithful builds."""
+    rng = np.random.default_rng(2025)
+    st = rng.normal(0.0, 1.0, (600, 4))
+    st[::7, 1] = st[::7, 0]
+    st[::11, 2] = st[::11, 1]
+    st[::13] = 0.0
+    st[::17, 3] = -st[::17, 2]
+    st[::19] = np.array([1.0, 2.0, 4.0, 8.0])
+    store["muscl/stencils"] = st
+    for lim in (0, 1, 2):
+        store[f"muscl/strict_L{lim}"] = STRICT.muscl(st, lim)
+        store[f"muscl/faithful_L{lim}"] = FAITHFUL.muscl(st, lim)
+    meta["muscl"] = {"limiters": {"0": "minmod", "1": "van Leer", "2": "superbee"}}
+
+
 def main():
     store: dict[str, np.ndarray] = {}
     meta: dict = {}
@@ -214,6 +233,7 @@ def main():
     gen_weno_large(meta, store)
     gen_dg(store, meta)
     gen_points(store, meta)
+    gen_muscl(store, meta)
     np.savez_compressed(HERE / "reference_golden.npz", **store)
     (HERE / "reference_golden.json").write_text(json.dumps(meta, indent=1, sort_keys=True))
     sz = (HERE / "reference_golden.npz").stat().st_size

@@ -140,3 +140,14 @@ def test_ghost_map_last_writer_rule(restatement):
     assert src[2, 5] == 5 * nx + 5   # row 2 reached from 3, 4, 5 -> 5 wins
     assert src[10, 5] == 8 * nx + 5
     assert src[0, 0] == -1 and kind[0, 0] == 1  # corner never filled
+
+
+def test_muscl_point_vectors(restatement, golden):
+    """MUSCL reconstruction (the reference's muscl_reconstruct, dead code in
+    its solvers and an option here): the restatement equals the strict
+    reference build bit for bit, and the Makefile-faithful build too."""
+    st = golden["muscl/stencils"]
+    for lim in (0, 1, 2):
+        out = restatement.muscl(st, lim)
+        np.testing.assert_array_equal(out, golden[f"muscl/strict_L{lim}"])
+        np.testing.assert_array_equal(out, golden[f"muscl/faithful_L{lim}"])

@@ -111,3 +111,29 @@ def test_centre_detonation_large_magnitudes():
     assert np.isfinite(mix).all()
     for q in range(4):
         assert rel_l1(mix[q], f64[q]) < 1e-6, q
+
+
+def test_tma_wait_timeout_is_reported_and_the_context_stays_usable():
+    """The mixed WENO kernel's bounded TMA wait, made to run out without any
+    fault: the barrier expects 16 bytes more than the copy delivers and the
+    wait gives up after one poll.  Every CTA records STATUS_TIMEOUT, settles
+    the missing bytes, lets its copy land and leaves without writing; the
+    state is untouched and the next steps give the bits of a fresh context."""
+    import ctypes as C
+    from zuikakucfd_b200 import Solver, _native as N, cases
+    c = cases.four_quadrant(64, seed=3)
+    U0 = c.conserved()
+    dt = cases.cfl_dt(c, 0.4)
+    with Solver(method="weno", precision="mixed") as s:
+        s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
+        s.set_state(U0)
+        st = C.c_uint32(0)
+        N.check(N.lib().zk_selftest_tma_timeout(s._h, 1, C.byref(st)))
+        assert st.value & 8, st.value
+        assert np.array_equal(s.get_state(), U0)
+        s.step(dt, 5)
+        out = s.get_state()
+        assert s.status_word() == 0
+    ref, st2 = run(c, dt, 5, "mixed")
+    assert st2 == 0
+    assert np.array_equal(out, ref)

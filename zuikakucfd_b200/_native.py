@@ -20,6 +20,7 @@ PRECISION = {"fp64": 0, "mixed": 1, "fp64_fma": 2}
 LIMITER = {"reference": 0, "none": 1, "tvb": 2, "tvb_mlp": 3}
 FLUX = {"hllc": 0, "hll": 1}
 BOUNDARY = {"exchange": 0, "periodic": 1}
+RECON = {"weno5": 0, "muscl_minmod": 1, "muscl_vanleer": 2, "muscl_superbee": 3}
 MLP_NPARAM = 3457
 MLP_IN = 40
 
@@ -35,7 +36,7 @@ class ZkError(RuntimeError):
 class zk_options(C.Structure):
     _fields_ = [("method", C.c_int), ("order", C.c_int), ("precision", C.c_int),
                 ("limiter", C.c_int), ("flux", C.c_int), ("boundary", C.c_int),
-                ("device", C.c_int), ("tvb_M", C.c_double)]
+                ("device", C.c_int), ("tvb_M", C.c_double), ("recon", C.c_int)]
 
 
 class zk_batch_options(C.Structure):
@@ -92,6 +93,7 @@ _SIGS = {
     "zk_limited_cells": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "zk_indicator_logits": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "zk_set_indicator_screen": (C.c_int, [_P, C.c_float]),
+    "zk_selftest_tma_timeout": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "zk_indicator_stage_features": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
     "zk_indicator_stage_logits": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                             C.POINTER(C.c_uint32)]),

@@ -541,6 +541,7 @@ int zk_batch_add(zk_batch* b, const zk_options* o, int ny, int nx, double da, do
         return bfail(ZK_ERR_ARG, "DG order must be 1..3, got %d", o->order);
     if (o->precision != ZK_PREC_FP64 && o->precision != ZK_PREC_MIXED)
         return bfail(ZK_ERR_ARG, "unknown precision %d", o->precision);
+    if (o->recon != ZK_RECON_WENO5) return bfail(ZK_ERR_UNSUPPORTED, "the batched runner reconstructs with WENO5 only");
     if (o->limiter < ZK_LIMITER_REFERENCE || o->limiter > ZK_LIMITER_TVB_MLP)
         return bfail(ZK_ERR_ARG, "unknown limiter %d", o->limiter);
     if (o->method == ZK_METHOD_DG && o->limiter >= ZK_LIMITER_TVB)

@@ -97,7 +97,7 @@ int zk_stage(zk_ctx* c, double dt, int stage) {
     double* in[3] = {c->Un, c->S1, c->S2};
     double* out[3] = {c->S1, c->S2, c->Un};
     e = zk::launch_weno_stage_f64(c->fma(), in[stage - 1], c->Un, out[stage - 1], c->kind, c->gsrc, c->g, dt / c->da,
-                                   dt / c->da, c->gamma, stage, c->d_status, c->stream);
+                                   dt / c->da, c->gamma, stage, c->d_status, c->stream, c->opt.recon);
     return e == cudaSuccess ? ZK_OK : cuda_fail(e);
 }
 

@@ -39,11 +39,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
-// Bounded wait on phase `phase`; false if the limit ran out.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
-    for (uint32_t i = 0; i < kSpinLimit; ++i)
+// Bounded wait on phase `phase` (at most `limit` polls); false if the limit
+// ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit = kSpinLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
+}
+
+// Counts `bytes` of the current phase's expected transaction as done (the
+// failure self-test settles the bytes it asked for but never sent).
+__device__ __forceinline__ void mbar_complete_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
 // 3D tiled TMA load global -> shared, completion counted on `bar`.

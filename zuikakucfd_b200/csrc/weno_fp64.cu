@@ -68,6 +68,40 @@ __device__ __forceinline__ void weno5(double UL2, double UL1, double UP, double 
     UR = (e0 * qR0 + e1 * qR1 + e2 * qR2) * inv2;
 }
 
+// muscl_reconstruct, src_WENO/fluid.cpp:203-225 (not called by the reference's
+// solvers; the ZK_RECON_MUSCL_* options): cells UL2, UL1 | UR1, UR2 around the
+// face, slopes through minmod (LIM 0), van Leer (1) or superbee (2).
+__device__ __forceinline__ double minmod2(double a, double b) {
+    return a * b <= 0.0 ? 0.0 : (fabs(a) < fabs(b) ? a : b);
+}
+template <int LIM>
+__device__ __forceinline__ double muscl_slope(double a, double b) {
+    if constexpr (LIM == 0) {
+        return minmod2(a, b);
+    } else if constexpr (LIM == 1) {
+        const double ab = a * b;
+        return ab <= 0.0 ? 0.0 : 2.0 * ab / (a + b);
+    } else {
+        const double s1 = minmod2(a, 2.0 * b), s2 = minmod2(2.0 * a, b);
+        return s1 * s2 <= 0.0 ? 0.0 : (fabs(s1) > fabs(s2) ? s1 : s2);
+    }
+}
+template <int LIM>
+__device__ __forceinline__ void muscl(double UL2, double UL1, double UR1, double UR2, double& UL, double& UR) {
+    const double dL = UL1 - UL2, dC = UR1 - UL1, dR = UR2 - UR1;
+    UL = UL1 + 0.5 * muscl_slope<LIM>(dL, dC);
+    UR = UR1 - 0.5 * muscl_slope<LIM>(dC, dR);
+}
+
+// Face states from the six cells a3 a2 a1 | b1 b2 b3 around a face: WENO5
+// (RECON 0, the reference's scheme) or MUSCL with limiter RECON - 1.
+template <int RECON>
+__device__ __forceinline__ void face_states(double a3, double a2, double a1, double b1, double b2, double b3,
+                                            double& UL, double& UR) {
+    if constexpr (RECON == 0) weno5(a3, a2, a1, b1, b2, b3, UL, UR);
+    else muscl<RECON - 1>(a2, a1, b1, b2, UL, UR);
+}
+
 // hllcFlux (WENO variant), src_WENO/fluid.cpp:268-317
 __device__ __forceinline__ void hllc(const double L[4], const double R[4], double gamma, double F[4]) {
     const double eps = 1e-12;
@@ -135,7 +169,7 @@ struct Smem {
 // One tile whose top-left cell is (i0, j0).  Ends with every thread past its
 // last shared-memory read, so a persistent caller may reuse S after a barrier.
 // Returns the thread's max wave speed of the cells it wrote (want_lam), else 0.
-template <int TY, int NW = TY + 1>
+template <int TY, int NW = TY + 1, int RECON = 0>
 __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0, Smem<TY>& S) {
     constexpr int HY = Tile<TY, NW>::HY, NWARP = Tile<TY, NW>::NWARP, NTHREAD = Tile<TY, NW>::NTHREAD;
     auto& sU = S.sU;
@@ -178,8 +212,8 @@ __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0,
             double QL[4], QR[4], F[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-                weno5(sU[q][r + 3][c], sU[q][r + 3][c + 1], sU[q][r + 3][c + 2], sU[q][r + 3][c + 3],
-                      sU[q][r + 3][c + 4], sU[q][r + 3][c + 5], QL[q], QR[q]);
+                face_states<RECON>(sU[q][r + 3][c], sU[q][r + 3][c + 1], sU[q][r + 3][c + 2], sU[q][r + 3][c + 3],
+                                   sU[q][r + 3][c + 4], sU[q][r + 3][c + 5], QL[q], QR[q]);
             hllc(QL, QR, a.gamma, F);
 #pragma unroll
             for (int q = 0; q < 4; ++q) sFx[q][r][c] = F[q];
@@ -191,8 +225,8 @@ __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0,
             double QL[4], QR[4], F[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-                weno5(sU[q][r][c + 3], sU[q][r + 1][c + 3], sU[q][r + 2][c + 3], sU[q][r + 3][c + 3],
-                      sU[q][r + 4][c + 3], sU[q][r + 5][c + 3], QL[q], QR[q]);
+                face_states<RECON>(sU[q][r][c + 3], sU[q][r + 1][c + 3], sU[q][r + 2][c + 3], sU[q][r + 3][c + 3],
+                                   sU[q][r + 4][c + 3], sU[q][r + 5][c + 3], QL[q], QR[q]);
             double L[4] = {QL[0], QL[2], QL[1], QL[3]}, R[4] = {QR[0], QR[2], QR[1], QR[3]};
             hllc(L, R, a.gamma, F);
 #pragma unroll
@@ -249,9 +283,10 @@ __device__ __forceinline__ double stage_tile(const StageArgs& a, int j0, int i0,
 }
 
 // 3 CTAs per SM (72 registers, no spills): +19% over 2 CTAs at 84 registers.
+template <int RECON>
 __global__ void __launch_bounds__(Tile<8>::NTHREAD, 3) weno_stage_fp64_kernel(StageArgs a) {
     __shared__ Smem<8> S;
-    stage_tile<8>(a, blockIdx.x * TX, blockIdx.y * 8, S);
+    stage_tile<8, 9, RECON>(a, blockIdx.x * TX, blockIdx.y * 8, S);
 }
 
 // Persistent stage over every listed problem of a batch group: CTA b takes
@@ -339,10 +374,16 @@ int weno_fp64_batch_occupancy(int variant) {
 cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
                                    const int8_t* kind, const int32_t* gsrc, const Grid& g,
                                    double dtdx, double dtdy, double gamma, int stage,
-                                   uint32_t* status, cudaStream_t s) {
+                                   uint32_t* status, cudaStream_t s, int recon) {
     StageArgs a{Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status};
     dim3 grid((g.nx + TX - 1) / TX, (g.ny + 7) / 8);
-    weno_stage_fp64_kernel<<<grid, Tile<8>::NTHREAD, 0, s>>>(a);
+    switch (recon) {
+        case 0: weno_stage_fp64_kernel<0><<<grid, Tile<8>::NTHREAD, 0, s>>>(a); break;
+        case 1: weno_stage_fp64_kernel<1><<<grid, Tile<8>::NTHREAD, 0, s>>>(a); break;
+        case 2: weno_stage_fp64_kernel<2><<<grid, Tile<8>::NTHREAD, 0, s>>>(a); break;
+        case 3: weno_stage_fp64_kernel<3><<<grid, Tile<8>::NTHREAD, 0, s>>>(a); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

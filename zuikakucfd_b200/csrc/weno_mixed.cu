@@ -175,6 +175,10 @@ struct MixedArgs {
     int stage;
     uint32_t* status;
     int want_lam;  // 1: report the max wave speed of the cells written
+    // failure self-test only (0 in every step): the barrier expects extra_tx
+    // bytes more than the copy delivers, and the wait gives up after `spin`
+    // polls (0: kSpinLimit)
+    uint32_t extra_tx, spin;
 };
 
 template <int TY>
@@ -259,15 +263,17 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
     // 1. TMA: the 40 x (TY+6) x 4 box starting at (j0-4, i0-3, 0); out-of-range
     //    elements arrive as zeros
     if (threadIdx.x == 0) {
-        mbar_arrive_expect_tx(bar, (uint32_t)sizeof(stg));
+        mbar_arrive_expect_tx(bar, (uint32_t)sizeof(stg) + a.extra_tx);
         tma_load_3d(&stg[0][0][0], tmap, bar, j0 - 4, i0 - 3, 0);
     }
-    const bool ok = mbar_wait_bounded(bar, phase);
+    const bool ok = mbar_wait_bounded(bar, phase, a.spin ? a.spin : kSpinLimit);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) {
             atomicOr(a.status, STATUS_TIMEOUT);
+            if (a.extra_tx) mbar_complete_tx(bar, a.extra_tx);  // self-test: settle the bytes never sent
             mbar_wait_bounded(bar, phase);  // give a late copy a second bounded chance to land
         }
+        __syncthreads();  // no thread leaves before the copy into this CTA's shared memory has landed
         return false;
     }
 
@@ -495,6 +501,19 @@ cudaError_t launch_weno_stage_mixed(const CUtensorMap& tmap, const double* Ucur,
     return cudaGetLastError();
 }
 
+// Stage 1 of the mixed WENO step with a barrier that expects 16 bytes more
+// than the TMA copy delivers and a wait limited to `spin` polls: every CTA
+// runs out of its wait, records STATUS_TIMEOUT, settles the missing bytes,
+// waits for its copy to land and leaves without writing its tile.
+cudaError_t launch_weno_timeout_selftest(const CUtensorMap& tmap, const double* Un, double* Uout, const int8_t* kind,
+                                         const int32_t* gsrc, const Grid& g, double dtdx, double dtdy, double gamma,
+                                         uint32_t spin, uint32_t* status, cudaStream_t s) {
+    MixedArgs a{Un, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, 1, status, 0, 16u, spin ? spin : 1u};
+    dim3 grid((g.nx + TX - 1) / TX, (g.ny + 7) / 8);
+    weno_stage_mixed_kernel<<<grid, Tile<8>::NTHREAD, 0, s>>>(tmap, a);
+    return cudaGetLastError();
+}
+
 // Tensor map over one FP64 WENO state: dims (x = nx, y = ny, field = 4),
 // strides pitch*8 and plane*8 bytes, box 40 x (rows + 6) x 4.
 bool encode_weno_state_map(CUtensorMap* m, const double* base, const Grid& g, const char** err, int rows) {
@@ -528,6 +547,21 @@ int zk_weno_mixed_step(zk_ctx* c, double dt) {
                                         3, c->d_status, c->stream);
     if (e != cudaSuccess) return zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
     return ZK_OK;
+}
+
+extern "C" int zk_selftest_tma_timeout(zk_ctx* c, uint32_t spin_limit, uint32_t* status_out) {
+    if (!c || !c->Un || !status_out) return zk_internal_fail(ZK_ERR_ARG, "needs a context with a mesh and status_out");
+    if (c->opt.method != ZK_METHOD_WENO || c->opt.precision != ZK_PREC_MIXED)
+        return zk_internal_fail(ZK_ERR_UNSUPPORTED, "needs a mixed-precision WENO context");
+    cudaError_t e = cudaSetDevice(c->opt.device);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess)
+        e = zk::launch_weno_timeout_selftest(c->tmap[0], c->Un, c->S1, c->kind, c->gsrc, c->g, 1e-6 / c->da,
+                                             1e-6 / c->da, c->gamma, spin_limit, c->d_status, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(status_out, c->d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? ZK_OK : zk_internal_fail(ZK_ERR_CUDA, cudaGetErrorString(e));
 }
 
 // Stage `stage` (1..3) of zk_weno_mixed_step alone: the same launch with the

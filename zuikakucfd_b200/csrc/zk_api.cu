@@ -126,6 +126,7 @@ void zk_default_options(zk_options* o) {
     o->boundary = ZK_BOUNDARY_EXCHANGE;
     o->device = 0;
     o->tvb_M = 50.0;
+    o->recon = ZK_RECON_WENO5;
 }
 
 int zk_version(void) { return 100; }
@@ -147,6 +148,10 @@ int zk_create(const zk_options* opt, zk_ctx** out) {
         return fail(ZK_ERR_ARG, "unknown flux %d", opt->flux);
     if (opt->boundary != ZK_BOUNDARY_EXCHANGE && opt->boundary != ZK_BOUNDARY_PERIODIC)
         return fail(ZK_ERR_ARG, "unknown boundary %d", opt->boundary);
+    if (opt->recon < ZK_RECON_WENO5 || opt->recon > ZK_RECON_MUSCL_SUPERBEE)
+        return fail(ZK_ERR_ARG, "unknown reconstruction %d", opt->recon);
+    if (opt->recon != ZK_RECON_WENO5 && (opt->method != ZK_METHOD_WENO || opt->precision == ZK_PREC_MIXED))
+        return fail(ZK_ERR_UNSUPPORTED, "MUSCL reconstruction runs on WENO contexts at FP64 / FP64_FMA precision");
     int ndev = 0;
     ZK_CUDA(cudaGetDeviceCount(&ndev));
     if (opt->device < 0 || opt->device >= ndev)
@@ -335,9 +340,9 @@ int zk_status_word(zk_ctx* c, uint32_t* out) {
 // One SSP-RK3 step of the WENO path on the device state (enqueue only).
 static int weno_step_fp64(zk_ctx* c, double dt) {
     const double dtdx = dt / c->da, dtdy = dt / c->da;
-    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 1, c->d_status, c->stream));
-    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S1, c->Un, c->S2, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 2, c->d_status, c->stream));
-    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S2, c->Un, c->Un, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 3, c->d_status, c->stream));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 1, c->d_status, c->stream, c->opt.recon));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S1, c->Un, c->S2, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 2, c->d_status, c->stream, c->opt.recon));
+    ZK_CUDA(launch_weno_stage_f64(c->fma(), c->S2, c->Un, c->Un, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 3, c->d_status, c->stream, c->opt.recon));
     return ZK_OK;
 }
 
@@ -444,7 +449,7 @@ int zk_rhs(zk_ctx* c, double dt, double* host_dU) {
         if (int rc = zk_dg_rhs(c, c->S1)) return rc;
     } else {
         const double dtdx = dt / c->da, dtdy = dt / c->da;
-        ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 0, c->d_status, c->stream));
+        ZK_CUDA(launch_weno_stage_f64(c->fma(), c->Un, c->Un, c->S1, c->kind, c->gsrc, c->g, dtdx, dtdy, c->gamma, 0, c->d_status, c->stream, c->opt.recon));
     }
     ZK_CUDA(cudaMemcpy2DAsync(host_dU, sizeof(double) * c->g.nx, c->S1, sizeof(double) * c->g.pitch,
                               sizeof(double) * c->g.nx, (size_t)c->nvar * c->g.ny,

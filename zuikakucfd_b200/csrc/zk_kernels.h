@@ -8,10 +8,11 @@
 namespace zk {
 
 // ---- FP64 reference-arithmetic kernels (built with --fmad=false) ----------
+// recon: ZK_RECON_* face reconstruction (0 = WENO5, the reference's scheme)
 cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
                                    const int8_t* kind, const int32_t* gsrc, const Grid& g,
                                    double dtdx, double dtdy, double gamma, int stage,
-                                   uint32_t* status, cudaStream_t s);
+                                   uint32_t* status, cudaStream_t s, int recon = 0);
 
 }  // namespace zk
 
@@ -21,7 +22,7 @@ namespace zk_fma {
 cudaError_t launch_weno_stage_fp64(const double* Ucur, const double* Un, double* Uout,
                                    const int8_t* kind, const int32_t* gsrc, const zk::Grid& g,
                                    double dtdx, double dtdy, double gamma, int stage,
-                                   uint32_t* status, cudaStream_t s);
+                                   uint32_t* status, cudaStream_t s, int recon = 0);
 }  // namespace zk_fma
 
 namespace zk {
@@ -30,9 +31,11 @@ namespace zk {
 // kernel, or (fma) the contracted one.
 inline cudaError_t launch_weno_stage_f64(bool fma, const double* Ucur, const double* Un, double* Uout,
                                          const int8_t* kind, const int32_t* gsrc, const Grid& g, double dtdx,
-                                         double dtdy, double gamma, int stage, uint32_t* status, cudaStream_t s) {
-    return fma ? zk_fma::launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s)
-               : launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s);
+                                         double dtdy, double gamma, int stage, uint32_t* status, cudaStream_t s,
+                                         int recon) {
+    return fma ? zk_fma::launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s,
+                                                recon)
+               : launch_weno_stage_fp64(Ucur, Un, Uout, kind, gsrc, g, dtdx, dtdy, gamma, stage, status, s, recon);
 }
 
 cudaError_t launch_fill_ghosts(double* U, const int8_t* kind, const int32_t* gsrc, const Grid& g,

@@ -31,7 +31,7 @@ class Solver:
 
     def __init__(self, method: str = "weno", order: int = 2, precision: str = "fp64",
                  limiter: str = "reference", flux: str = "hllc", boundary: str = "exchange",
-                 device: int = 0, tvb_M: float = 50.0):
+                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5"):
         L = N.lib()
         o = N.zk_options()
         L.zk_default_options(C.byref(o))
@@ -43,6 +43,7 @@ class Solver:
         o.boundary = N.BOUNDARY[boundary]
         o.device = int(device)
         o.tvb_M = float(tvb_M)
+        o.recon = N.RECON[recon]
         h = C.c_void_p()
         N.check(L.zk_create(C.byref(o), C.byref(h)))
         self._h = h
@@ -225,7 +226,7 @@ class Mesh:
 
     def __init__(self, *args, method: str = "weno", order: int = 2, precision: str = "fp64",
                  limiter: str = "reference", flux: str = "hllc", boundary: str = "exchange",
-                 device: int = 0, tvb_M: float = 50.0):
+                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5"):
         self.method, self.order = method, int(order)
         self._opts = dict(method=method, order=order, precision=precision, limiter=limiter,
                           flux=flux, boundary=boundary, device=device, tvb_M=tvb_M)
