@@ -49,10 +49,14 @@ FLOPS_PER_CELL_STAGE = {("weno", 0): WENO_FLOPS_PER_CELL_STAGE, ("dg", 1): 1700.
 
 
 # DRAM bytes per launch of the dominant kernel, from an ncu capture
-# (dram__bytes_read.sum + dram__bytes_write.sum) of a small instance of the
-# workload, scaled to a full launch by the updated cells; None where not
-# captured.  Keyed by (workload, precision).
-KERNEL_TRAFFIC: dict = {}
+# (dram__bytes_read.sum + dram__bytes_write.sum) of a 512^2 instance of the
+# workload (256,036 updated cells), scaled to a full launch by the updated
+# cells; None where not captured.  Keyed by (workload, precision):
+# (bytes per updated cell, what was captured).
+KERNEL_TRAFFIC_PER_CELL: dict = {
+    ("dg3_fq_2048", "mixed"): (977.2, "dg_stage_mixed_pair_kernel<3,float,float,MLP> (stage 2) at 512^2: "
+                                      "201.8 MB read + 48.3 MB written"),
+}
 
 
 def make_workload(name: str, rank: int):
@@ -374,7 +378,12 @@ def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: 
             kname += ", FMA-contracted build"
         roofs[prec] = {
             "bound": "fp64" if f64 else "fp32", "achieved": achieved, "peak": pk,
-            "unit": "TFLOP/s", "frac": achieved / pk, "traffic": KERNEL_TRAFFIC.get((name, prec)),
+            "unit": "TFLOP/s", "frac": achieved / pk,
+            "traffic": (KERNEL_TRAFFIC_PER_CELL[(name, prec)][0] * cells
+                        if (name, prec) in KERNEL_TRAFFIC_PER_CELL else None),
+            "traffic_source": (KERNEL_TRAFFIC_PER_CELL[(name, prec)][1] + ", scaled by updated cells"
+                               if (name, prec) in KERNEL_TRAFFIC_PER_CELL else None),
+            "algorithmic_bytes": hbm_bytes,
             "kernel": kname, "flops_per_cell_stage": fl,
             "avg_launch_ms": stage_ms,
             "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU "
