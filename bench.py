@@ -375,7 +375,8 @@ def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: 
             kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if f64
                      else "dg_stage_mixed_pair_kernel" if w["order"] >= 2 else "dg_stage_mixed_kernel")
         if prec == "fp64_fma":
-            kname += ", FMA-contracted build"
+            kname = ("weno_stage_fp64_kernel, FMA-contracted build" if w["method"] == "weno"
+                     else "dg_stage_fused_fp64_kernel (one fused FP64 launch per stage, FMA)")
         roofs[prec] = {
             "bound": "fp64" if f64 else "fp32", "achieved": achieved, "peak": pk,
             "unit": "TFLOP/s", "frac": achieved / pk,

@@ -46,7 +46,8 @@ enum { ZK_METHOD_WENO = 0, ZK_METHOD_DG = 1 };
  * with FP64 conserved-state accumulation and FP64 pressure recovery.
  * FP64_FMA: FP64 throughout with multiply-adds fused, as the reference's own
  * Makefile build contracts them (within 1e-10 of that build, not bit-identical;
- * single contexts only, not the batched runner). */
+ * single contexts only, not the batched runner); DG stages run as one fused,
+ * sum-factorised kernel per stage, the FP64 twin of the mixed-precision one. */
 enum { ZK_PREC_FP64 = 0, ZK_PREC_MIXED = 1, ZK_PREC_FP64_FMA = 2 };
 /* DG limiter: REFERENCE = Persson modal filter + Zhang-Shu positivity
  * (src_DG/fluid.cpp:824-992); NONE; TVB = Cockburn-Shu TVB minmod (M) with

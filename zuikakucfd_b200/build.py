@@ -45,6 +45,7 @@ SOURCES: list[tuple] = [
     ("dg_fp64.cu", FMA, "dg_fp64_fma.o"),
     ("dg_driver.cu", []),
     ("dg_mixed.cu", ["--use_fast_math"]),
+    ("dg_fused_fp64.cu", []),
     ("dg_tvb.cu", STRICT),
     ("mlp.cu", []),
     ("peak.cu", []),

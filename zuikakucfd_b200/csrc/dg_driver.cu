@@ -28,6 +28,10 @@ cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const dou
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
                                   const FusedIndicator* ind, cudaStream_t s);
 bool dg_mixed_fuses_indicator(int P);
+int dg_upload_sep_f64(int P);
+cudaError_t launch_dg_stage_fused_fp64(int P, const double* cur, const double* un, double* out, const int8_t* kind,
+                                       const int32_t* gsrc, const Grid& g, double dt, double da, double gamma,
+                                       int stage, int limiter, int hll, double s0, uint32_t* status, cudaStream_t s);
 }  // namespace zk
 
 namespace zk_fma {  // dg_fp64.cu compiled with fused multiply-adds (ZK_PREC_FP64_FMA)
@@ -38,8 +42,14 @@ int dg_upload_tables(int P, const zk::DGTab& T);
 
 namespace {
 
-// The FP64 stage / reference limiter of a context's precision.
+// The FP64 stage / reference limiter of a context's precision: the
+// reference-arithmetic launches, or with FMA contraction the fused FP64 stage
+// kernel (dg_fused_fp64.cu; stages 1-3) and the contracted build of the
+// reference-arithmetic kernels (the RHS alone, stage 0).
 cudaError_t stage_f64(zk_ctx* c, const zk::DGArgs& a) {
+    if (c->fma() && a.stage >= 1)
+        return zk::launch_dg_stage_fused_fp64(c->opt.order, a.cur, a.un, a.out, a.kind, a.gsrc, a.g, a.dt, c->da,
+                                              a.gamma, a.stage, a.limiter, a.hll, a.s0, a.status, c->stream);
     return c->fma() ? zk_fma::launch_dg_stage_fp64(c->opt.order, a, c->stream)
                     : zk::launch_dg_stage_fp64(c->opt.order, a, c->stream);
 }
@@ -130,7 +140,7 @@ int zk_dg_setup(zk_ctx* c) {
     double phic[zk::DG_MAXNM * 4];
     zk::dg_make_tables(P, &tab, phic);
     if (zk::dg_upload_tables(P, tab) != ZK_OK) return zk_internal_fail(ZK_ERR_CUDA, "DG table upload failed");
-    if (c->fma() && zk_fma::dg_upload_tables(P, tab) != ZK_OK)
+    if (c->fma() && (zk_fma::dg_upload_tables(P, tab) != ZK_OK || zk::dg_upload_sep_f64(P) != ZK_OK))
         return zk_internal_fail(ZK_ERR_CUDA, "DG table upload failed");
     s->s0 = (P >= 3) ? -3.0 * std::log10((double)P) : -4.0 * std::log10((double)P);
     s->xpitch = c->g.pitch + 32;
