@@ -436,7 +436,7 @@ def main():
     ap.add_argument("--workload", default="dg3_fq_2048")
     ap.add_argument("--secondary", default="weno_fq_2048,batch64",
                     help="comma-separated workloads measured after the headline into the line's "
-                         "'secondary' object ('' for none)")
+                         "'secondary' object ('none' for none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-refined", action="store_true", help="skip the refined-solution L1 study")
@@ -472,7 +472,7 @@ def main():
                               cpu_seconds=15.0 if primary else 8.0, refined=not args.no_refined)
 
     out = one(args.workload, True)
-    sec = [n for n in args.secondary.split(",") if n and n != args.workload]
+    sec = [n for n in args.secondary.split(",") if n and n not in (args.workload, "none")]
     if sec:
         res = {n: one(n, False) for n in sec}
         if rank == 0:

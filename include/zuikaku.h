@@ -76,6 +76,8 @@ typedef struct zk_options {
     int device;     /* CUDA device ordinal                   */
     double tvb_M;   /* TVB constant M (default 50)           */
     int recon;      /* ZK_RECON_* (WENO only; default WENO5) */
+    int tile_tpc;   /* mixed DG: threads per cell of the stage kernel, 1 or 2;
+                       0 (default) = chosen by timing both on the first step */
 } zk_options;
 
 typedef struct zk_ctx zk_ctx;
@@ -143,6 +145,10 @@ int zk_synchronize(zk_ctx* ctx);
 /* Timing helper: runs nsteps steps and returns the device time measured with
  * CUDA events on the context's stream. */
 int zk_step_timed(zk_ctx* ctx, double dt, int nsteps, float* ms);
+
+/* Threads per cell the mixed DG stage kernel of this context runs (1 or 2;
+ * 0 before the first step).  No counterpart in the reference. */
+int zk_tile_tpc(zk_ctx* ctx, int* tpc);
 
 /* Device pointer of the FP64 state (layout: planes of ny rows x pitch
  * doubles) and its row pitch in elements, for zero-copy callers. */

@@ -137,3 +137,33 @@ def test_l2_projected_wave_convergence_and_mixed_error():
         assert errs[n][1] <= max(1.1 * errs[n][0], 2e-7), (n, errs[n])
     order = np.log2(errs[32][0] / errs[64][0])
     assert order > 2.5, (order, errs)
+
+
+@pytest.mark.parametrize("P,limiter", [(1, "reference"), (2, "tvb"), (3, "reference"), (3, "tvb")])
+def test_single_path_threads_per_cell_choices_give_identical_bits(P, limiter):
+    """The single-problem mixed stage with one and with two threads per cell
+    (pinned through tile_tpc) and with the choice left to the autotuner gives
+    the same bits; the tuner reports what it chose."""
+    from zuikakucfd_b200 import Solver, cases
+    c = cases.four_quadrant(70, seed=3, ny=45)
+    dt = dg_dt(P, c)
+    outs = {}
+    for tpc in (1, 2, 0):
+        with Solver(method="dg", order=P, precision="mixed", limiter=limiter, tile_tpc=tpc) as s:
+            s.set_mesh(c.ny, c.nx, c.da, c.gamma, c.bctype)
+            s.set_state(c.dg_state(P))
+            assert s.tile_tpc() == 0
+            s.step(dt, 8)
+            outs[tpc] = s.get_state()
+            chosen = s.tile_tpc()
+            assert chosen == tpc if tpc else chosen in (1, 2)
+            assert s.status_word() == 0
+    assert np.array_equal(outs[1], outs[2])
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_fused_indicator_needs_two_threads_per_cell():
+    from zuikakucfd_b200 import Solver
+    from zuikakucfd_b200._native import ZkError
+    with pytest.raises(ZkError, match="two threads per cell"):
+        Solver(method="dg", order=3, precision="mixed", limiter="tvb_mlp", tile_tpc=1)

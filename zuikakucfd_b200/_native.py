@@ -36,7 +36,7 @@ class ZkError(RuntimeError):
 class zk_options(C.Structure):
     _fields_ = [("method", C.c_int), ("order", C.c_int), ("precision", C.c_int),
                 ("limiter", C.c_int), ("flux", C.c_int), ("boundary", C.c_int),
-                ("device", C.c_int), ("tvb_M", C.c_double), ("recon", C.c_int)]
+                ("device", C.c_int), ("tvb_M", C.c_double), ("recon", C.c_int), ("tile_tpc", C.c_int)]
 
 
 class zk_batch_options(C.Structure):
@@ -93,6 +93,7 @@ _SIGS = {
     "zk_limited_cells": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "zk_indicator_logits": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "zk_set_indicator_screen": (C.c_int, [_P, C.c_float]),
+    "zk_tile_tpc": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "zk_selftest_tma_timeout": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint32)]),
     "zk_indicator_stage_features": (C.c_int, [_P, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
     "zk_indicator_stage_logits": (C.c_int, [_P, C.c_double, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),

@@ -3,6 +3,9 @@
 #include <cmath>
 #include <cstring>
 
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include <cuda_bf16.h>
@@ -26,8 +29,9 @@ cudaError_t launch_dg_tvb_list(int P, void* state, bool fp64, const int8_t* kind
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
-                                  const FusedIndicator* ind, cudaStream_t s);
+                                  const FusedIndicator* ind, int tpc, cudaStream_t s);
 bool dg_mixed_fuses_indicator(int P);
+int dg_mixed_default_tpc(int P);
 int dg_upload_sep_f64(int P);
 cudaError_t launch_dg_stage_fused_fp64(int P, const double* cur, const double* un, double* out, const int8_t* kind,
                                        const int32_t* gsrc, const Grid& g, double dt, double da, double gamma,
@@ -125,7 +129,64 @@ cudaError_t mixed_stage(zk_ctx* c, double dt, int stage, float* dbg = nullptr) {
                            (uint32_t)c->g.plane, dbg, c->mlp_screen};
     return zk::launch_dg_stage_mixed(c->opt.order, io.in, io.in64, c->Un, io.out, io.out64, c->kind, c->gsrc, c->g,
                                      dt, c->da, c->gamma, stage, c->opt.limiter, c->opt.flux == ZK_FLUX_HLL,
-                                     st(c)->s0, c->d_status, fused_indicator(c) ? &ind : nullptr, c->stream);
+                                     st(c)->s0, c->d_status, fused_indicator(c) ? &ind : nullptr, c->dg_tpc,
+                                     c->stream);
+}
+
+// Threads per cell of the mixed stage kernel: pinned (opt.tile_tpc), two with
+// the fused indicator, else tuned once per (device, order, grid) by timing
+// stage 1 of each choice on this context's state (both give the same bits;
+// the timing launches write only the stage-1 buffer, which the step then
+// rewrites).  Skipped, with the default, while the stream is being captured.
+int choose_tpc(zk_ctx* c, double dt) {
+    using Key = std::tuple<int, int, int, int>;
+    static std::mutex mu;
+    static std::map<Key, int> cache;
+    if (c->opt.tile_tpc == 1 || c->opt.tile_tpc == 2) {
+        c->dg_tpc = c->opt.tile_tpc;
+        return ZK_OK;
+    }
+    if (fused_indicator(c)) {
+        c->dg_tpc = 2;
+        return ZK_OK;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        c->dg_tpc = zk::dg_mixed_default_tpc(c->opt.order);
+        return ZK_OK;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Key key{dev, c->opt.order, c->g.ny, c->g.nx};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            c->dg_tpc = it->second;
+            return ZK_OK;
+        }
+    }
+    float best = 0.0f;
+    int best_tpc = zk::dg_mixed_default_tpc(c->opt.order);
+    for (int tpc : {1, 2}) {
+        c->dg_tpc = tpc;
+        cudaError_t e = mixed_stage(c, dt, 1);  // first use (and warm-up)
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev0, c->stream);
+        for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = mixed_stage(c, dt, 1);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev1, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev1);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        if (e != cudaSuccess) return cuda_fail(e);
+        if (tpc == 1 || ms < best) {
+            best = ms;
+            best_tpc = tpc;
+        }
+    }
+    c->dg_tpc = best_tpc;
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = best_tpc;
+    return ZK_OK;
 }
 
 }  // namespace
@@ -230,6 +291,8 @@ void zk_dg_release(zk_ctx* c) {
 }
 
 static int dg_step_mixed(zk_ctx* c, double dt) {
+    if (!c->dg_tpc)
+        if (int rc = choose_tpc(c, dt)) return rc;
     if (int rc = begin_step(c)) return rc;
     for (int k = 1; k <= 3; ++k) {
         const cudaError_t e = mixed_stage(c, dt, k);
@@ -256,6 +319,8 @@ int zk_dg_step(zk_ctx* c, double dt) {
 // the same launch with the same buffers (FP64: U^n -> S1 -> S2 -> U^n;
 // mixed: U^n -> F1 -> F2 -> U^n).
 int zk_dg_stage(zk_ctx* c, double dt, int stage) {
+    if (c->opt.precision == ZK_PREC_MIXED && !c->dg_tpc)
+        if (int rc = choose_tpc(c, dt)) return rc;
     if (stage == 1)
         if (int rc = begin_step(c)) return rc;
     cudaError_t e;
@@ -456,5 +521,11 @@ extern "C" int zk_indicator_stage_logits(zk_ctx* c, double dt, int stage, float*
             if (features) std::memcpy(features + cell * zk::MLP_IN, src, sizeof(float) * zk::MLP_IN);
             if (logits) logits[cell] = src[40];
         }
+    return ZK_OK;
+}
+
+extern "C" int zk_tile_tpc(zk_ctx* c, int* tpc) {
+    if (!c || !tpc) return zk_internal_fail(ZK_ERR_ARG, "null argument");
+    *tpc = c->dg_tpc;
     return ZK_OK;
 }

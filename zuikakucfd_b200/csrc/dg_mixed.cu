@@ -1373,9 +1373,10 @@ __global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P, MLP>()
     stage_tile_pair<P, TIn, TOut, kPairRows, false, MLP>(a, blockIdx.x * MTX, blockIdx.y * kPairRows, smem);
 }
 
-// Threads per cell of the single-problem stage kernel, per P (measured at
-// 2048^2, four-quadrant, GDOF/s, one vs two threads per cell): P = 1 38.4 vs
-// 35.9, P = 2 39.0 vs 42.5, P = 3 33.8 vs 39.0.
+// Default threads per cell of the single-problem stage kernel, per P, when
+// the autotuner does not run (measured at 2048^2, four-quadrant, GDOF/s, one
+// vs two threads per cell): P = 1 38.4 vs 35.9, P = 2 39.0 vs 42.5, P = 3 33.8
+// vs 39.0.  The context's autotuner times both on its own grid (dg_driver.cu).
 constexpr int kSingleTpc[4] = {0, 1, 2, 2};
 
 // Persistent stage STAGE over every listed problem of a batch group, tile
@@ -1471,9 +1472,9 @@ cudaError_t batch_p(int variant, int stage, const DgItem* items, const int* dir,
     }
 }
 
-template <int P, typename TIn, typename TOut, bool MLP>
+template <int P, typename TIn, typename TOut, int TPC, bool MLP>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
-    constexpr bool pair = kSingleTpc[P] == 2;
+    constexpr bool pair = TPC == 2;
     static_assert(pair || !MLP, "the fused indicator runs in the two-threads-per-cell kernel");
     constexpr int rows = pair ? kPairRows : 4;
     constexpr size_t sm = pair ? pair_smem_bytes<P, MLP>() : smem_bytes<P, rows>();
@@ -1487,23 +1488,23 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
         attr_set[dev] = true;
     }
     dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + rows - 1) / rows);
-    kern<<<grid, MTX * rows * kSingleTpc[P], sm, s>>>(a);
+    kern<<<grid, MTX * rows * TPC, sm, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int P, typename TIn, typename TOut>
-cudaError_t launch_io(const MixArgs& a, cudaStream_t s) {
-    if constexpr (kSingleTpc[P] == 2)
-        if (a.mlp) return launch_one<P, TIn, TOut, true>(a, s);
-    return launch_one<P, TIn, TOut, false>(a, s);
+cudaError_t launch_io(const MixArgs& a, int tpc, cudaStream_t s) {
+    if constexpr (P >= 2)
+        if (a.mlp) return launch_one<P, TIn, TOut, 2, true>(a, s);
+    return tpc == 2 ? launch_one<P, TIn, TOut, 2, false>(a, s) : launch_one<P, TIn, TOut, 1, false>(a, s);
 }
 
 template <int P>
-cudaError_t launch_p(const MixArgs& a, int in_fp64, int out_fp64, cudaStream_t s) {
-    if (in_fp64 && !out_fp64) return launch_io<P, double, float>(a, s);
-    if (!in_fp64 && !out_fp64) return launch_io<P, float, float>(a, s);
-    if (!in_fp64 && out_fp64) return launch_io<P, float, double>(a, s);
-    return launch_io<P, double, double>(a, s);
+cudaError_t launch_p(const MixArgs& a, int in_fp64, int out_fp64, int tpc, cudaStream_t s) {
+    if (in_fp64 && !out_fp64) return launch_io<P, double, float>(a, tpc, s);
+    if (!in_fp64 && !out_fp64) return launch_io<P, float, float>(a, tpc, s);
+    if (!in_fp64 && out_fp64) return launch_io<P, float, double>(a, tpc, s);
+    return launch_io<P, double, double>(a, tpc, s);
 }
 
 }  // namespace
@@ -1576,19 +1577,22 @@ int dg_mixed_batch_tiles(int variant, int ny, int nx) {
 // One mixed-precision DG stage: cur (double if in_fp64 else float) -> out
 // (double if out_fp64 else float).
 
-// Whether the single-problem stage of order P can run the fused indicator.
-bool dg_mixed_fuses_indicator(int P) { return P >= 1 && P <= 3 && kSingleTpc[P] == 2; }
+// Whether the single-problem stage of order P runs the indicator fused (the
+// two-threads-per-cell kernel, P = 2, 3), and its default threads per cell.
+bool dg_mixed_fuses_indicator(int P) { return P >= 2 && P <= 3; }
+int dg_mixed_default_tpc(int P) { return P >= 1 && P <= 3 ? kSingleTpc[P] : 1; }
 // With `ind` (P = 2, 3: the two-threads-per-cell kernels) the learned
 // indicator runs fused in the stage and appends the cells it flags to
 // ind->list; the caller then runs the TVB list pass.
 cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const double* un, void* out, int out_fp64,
                                   const int8_t* kind, const int32_t* gsrc, const Grid& g, double dt, double da,
                                   double gamma, int stage, int limiter, int hll, double s0, uint32_t* status,
-                                  const FusedIndicator* ind, cudaStream_t s) {
+                                  const FusedIndicator* ind, int tpc, cudaStream_t s) {
     MixArgs a{cur, un, out, kind, gsrc, g, dt, (float)(0.5 / da), (float)gamma, stage, limiter, hll, (float)s0,
               status};
+    if (tpc != 1 && tpc != 2) tpc = dg_mixed_default_tpc(P);
     if (ind) {
-        if (kSingleTpc[P < 1 || P > 3 ? 0 : P] != 2) return cudaErrorInvalidValue;
+        if (!dg_mixed_fuses_indicator(P)) return cudaErrorInvalidValue;
         a.mlp = static_cast<const MlpFrag*>(ind->mlp);
         a.list = ind->list;
         a.count = ind->count;
@@ -1597,9 +1601,9 @@ cudaError_t launch_dg_stage_mixed(int P, const void* cur, int in_fp64, const dou
         a.screen = ind->screen;
     }
     switch (P) {
-        case 1: return launch_p<1>(a, in_fp64, out_fp64, s);
-        case 2: return launch_p<2>(a, in_fp64, out_fp64, s);
-        case 3: return launch_p<3>(a, in_fp64, out_fp64, s);
+        case 1: return launch_p<1>(a, in_fp64, out_fp64, tpc, s);
+        case 2: return launch_p<2>(a, in_fp64, out_fp64, tpc, s);
+        case 3: return launch_p<3>(a, in_fp64, out_fp64, tpc, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -127,6 +127,7 @@ void zk_default_options(zk_options* o) {
     o->device = 0;
     o->tvb_M = 50.0;
     o->recon = ZK_RECON_WENO5;
+    o->tile_tpc = 0;
 }
 
 int zk_version(void) { return 100; }
@@ -150,6 +151,10 @@ int zk_create(const zk_options* opt, zk_ctx** out) {
         return fail(ZK_ERR_ARG, "unknown boundary %d", opt->boundary);
     if (opt->recon < ZK_RECON_WENO5 || opt->recon > ZK_RECON_MUSCL_SUPERBEE)
         return fail(ZK_ERR_ARG, "unknown reconstruction %d", opt->recon);
+    if (opt->tile_tpc < 0 || opt->tile_tpc > 2) return fail(ZK_ERR_ARG, "tile_tpc must be 0, 1 or 2");
+    if (opt->tile_tpc == 1 && opt->limiter == ZK_LIMITER_TVB_MLP && opt->method == ZK_METHOD_DG && opt->order >= 2 &&
+        opt->precision == ZK_PREC_MIXED)
+        return fail(ZK_ERR_UNSUPPORTED, "the fused learned indicator runs two threads per cell");
     if (opt->recon != ZK_RECON_WENO5 && (opt->method != ZK_METHOD_WENO || opt->precision == ZK_PREC_MIXED))
         return fail(ZK_ERR_UNSUPPORTED, "MUSCL reconstruction runs on WENO contexts at FP64 / FP64_FMA precision");
     int ndev = 0;

@@ -41,6 +41,7 @@ struct zk_ctx {
     void* mlp_frag = nullptr;     // device MlpFrag (the same weights for the indicator fused in the stage)
     bool mlp_set = false;
     float mlp_screen = -1.0f;     // indicator screen (zk_set_indicator_screen); < 0: every cell evaluated
+    int dg_tpc = 0;               // threads per cell of the mixed DG stage kernel (0: not chosen yet)
     int32_t* d_list = nullptr;    // cells the fused indicator flagged in the current stage (pitched indices)
     uint32_t* d_lcount = nullptr; // their counts, one per RK stage, cleared at each step's stage 1
     uint8_t* d_flags = nullptr;   // TVB troubled-cell flags of the last pass, pitched

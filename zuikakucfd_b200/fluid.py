@@ -31,7 +31,7 @@ class Solver:
 
     def __init__(self, method: str = "weno", order: int = 2, precision: str = "fp64",
                  limiter: str = "reference", flux: str = "hllc", boundary: str = "exchange",
-                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5"):
+                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5", tile_tpc: int = 0):
         L = N.lib()
         o = N.zk_options()
         L.zk_default_options(C.byref(o))
@@ -44,6 +44,7 @@ class Solver:
         o.device = int(device)
         o.tvb_M = float(tvb_M)
         o.recon = N.RECON[recon]
+        o.tile_tpc = int(tile_tpc)
         h = C.c_void_p()
         N.check(L.zk_create(C.byref(o), C.byref(h)))
         self._h = h
@@ -140,6 +141,12 @@ class Solver:
             screen = indicator.load_screen() if params is None else -1.0
         N.check(N.lib().zk_set_indicator_screen(self._h, float(screen)))
 
+    def tile_tpc(self) -> int:
+        """Threads per cell of the mixed DG stage kernel (0 before the first step)."""
+        v = C.c_int()
+        N.check(N.lib().zk_tile_tpc(self._h, C.byref(v)))
+        return int(v.value)
+
     def status_word(self) -> int:
         v = C.c_uint32()
         N.check(N.lib().zk_status_word(self._h, C.byref(v)))
@@ -226,10 +233,11 @@ class Mesh:
 
     def __init__(self, *args, method: str = "weno", order: int = 2, precision: str = "fp64",
                  limiter: str = "reference", flux: str = "hllc", boundary: str = "exchange",
-                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5"):
+                 device: int = 0, tvb_M: float = 50.0, recon: str = "weno5", tile_tpc: int = 0):
         self.method, self.order = method, int(order)
         self._opts = dict(method=method, order=order, precision=precision, limiter=limiter,
-                          flux=flux, boundary=boundary, device=device, tvb_M=tvb_M)
+                          flux=flux, boundary=boundary, device=device, tvb_M=tvb_M, recon=recon,
+                          tile_tpc=tile_tpc)
         self.nm = (self.order + 1) ** 2 if method == "dg" else 1
         if len(args) == 1:
             c = read_case(args[0])
@@ -472,7 +480,7 @@ def loadCheckpoint(path: str | os.PathLike, **overrides) -> tuple[Mesh, float, i
     opts = {}
     for item in z["options"]:
         k, v = str(item).split("=", 1)
-        opts[k] = int(v) if k in ("order", "device") else float(v) if k == "tvb_M" else v
+        opts[k] = int(v) if k in ("order", "device", "tile_tpc") else float(v) if k == "tvb_M" else v
     opts.update(overrides)
     ny, nx = (int(x) for x in z["grid"])
     m = Mesh(ny, nx, float(z["da"]), float(z["gamma"]), **opts)
