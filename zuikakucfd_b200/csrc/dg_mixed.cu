@@ -53,6 +53,9 @@ __constant__ DGSepF c_sepf[3];
 // A tile is 32 x MTY cells with one thread per cell; shared memory holds the
 // tile plus a 1-cell halo (SX x (MTY + 2) slots).
 constexpr int MTX = 32, SX = MTX + 2;
+// U^n values a thread loads together in the combine of a stage with an FP64
+// output (U^(n+1) written over U^n)
+constexpr int kUnChunk = 8;
 
 struct MixArgs {
     const void* cur;  // stage input: double (stage 1: U^n) or float (U^(1), U^(2))
@@ -572,18 +575,30 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     const float* pw = sd + slot * VP;
     TOut* out = static_cast<TOut*>(a.out);
     constexpr bool OUT64 = sizeof(TOut) == 8;
+    // U^n in chunks loaded before any is combined (as stage_tile_pair: an
+    // FP64 output is U^n itself, and each store orders the loads after it);
+    // FP32-output chunks of 16 (64 values at once spill at 168 registers)
+    constexpr int UC = OUT64 ? kUnChunk : 16;
 #pragma unroll
-    for (int v4 = 0; v4 < 4 * NM; v4 += 4) {
-        const float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
-        const float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+    for (int v0 = 0; v0 < 4 * NM; v0 += UC) {
+        double unc[UC];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int v = v4 + e, q = v / NM, m = v % NM;
-            const double un = a.un[(size_t)v * plane + k];
-            const double du = (double)acc[q][m];
-            const double o = a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
-            acc[q][m] = (float)o;
-            if (OUT64) out[(size_t)v * plane + k] = (TOut)o;
+        for (int e = 0; e < UC; ++e)
+            if (v0 + e < 4 * NM) unc[e] = a.un[(size_t)(v0 + e) * plane + k];
+#pragma unroll
+        for (int v4 = v0; v4 < v0 + UC && v4 < 4 * NM; v4 += 4) {
+            const float4 c4 = *reinterpret_cast<const float4*>(pw + v4);
+            const float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int v = v4 + e, q = v / NM, m = v % NM;
+                const double un = unc[v - v0];
+                const double du = (double)acc[q][m];
+                const double o =
+                    a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
+                acc[q][m] = (float)o;
+                if (OUT64) out[(size_t)v * plane + k] = (TOut)o;
+            }
         }
     }
 
@@ -1121,20 +1136,35 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     TOut* out = static_cast<TOut*>(a.out);
     constexpr bool OUT64 = sizeof(TOut) == 8;
     double om[2] = {0.0, 0.0};  // this half's written cell means
+    // U^n in chunks of UC values loaded before any is combined: an FP64
+    // output is U^n itself, so each store orders the loads after it and a
+    // load per store is one L2 round trip per value (stage 3 at 2048^2, P = 3:
+    // 2.66 -> 1.93 ms).  With an FP32 output all of this half's values are
+    // loaded first (the P = 3 step: 5.75 -> 5.62 ms against a vector at a time)
+    constexpr int NV = 2 * NM, UC = OUT64 ? kUnChunk : NV;
+    static_assert(UC % VW == 0, "chunks of whole vectors");
 #pragma unroll
-    for (int v = 0; v < 2 * NM; v += VW) {
-        float cv[VW];
-        load_vec<VW>(pw + v, cv);
+    for (int v0 = 0; v0 < NV; v0 += UC) {
+        double unc[UC];
 #pragma unroll
-        for (int e = 0; e < VW; ++e) {
-            const int vv = v + e, cc = vv / NM, m = vv % NM;
-            const double un = a.un[(size_t)(2 * h * NM + vv) * plane + k];
-            const double du = (double)acc[cc][m];
-            const double o = a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
-            acc[cc][m] = (float)o;
-            if (OUT64) {
-                out[(size_t)(2 * h * NM + vv) * plane + k] = (TOut)o;
-                if (m == 0) om[cc] = o;
+        for (int e = 0; e < UC; ++e)
+            if (v0 + e < NV) unc[e] = a.un[(size_t)(2 * h * NM + v0 + e) * plane + k];
+#pragma unroll
+        for (int v = v0; v < v0 + UC && v < NV; v += VW) {
+            float cv[VW];
+            load_vec<VW>(pw + v, cv);
+#pragma unroll
+            for (int e = 0; e < VW; ++e) {
+                const int vv = v + e, cc = vv / NM, m = vv % NM;
+                const double un = unc[vv - v0];
+                const double du = (double)acc[cc][m];
+                const double o =
+                    a.stage == 1 ? __fma_rn(dt, du, un) : so_combine(a.stage, un, __fma_rn(dt, du, (double)cv[e]));
+                acc[cc][m] = (float)o;
+                if (OUT64) {
+                    out[(size_t)(2 * h * NM + vv) * plane + k] = (TOut)o;
+                    if (m == 0) om[cc] = o;
+                }
             }
         }
     }
