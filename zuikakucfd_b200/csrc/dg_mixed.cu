@@ -353,6 +353,57 @@ __device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* 
     }
 }
 
+// The tile (top-left cell (i0, j0)) and its 1-cell halo into shared memory,
+// ghosts taken from their source cells (slip walls negate the normal
+// momentum), slots outside the grid zero; the kind of every slot into sk.
+// One slot per thread; the input (FP64 or FP32) goes through registers, all
+// of a slot's loads in flight at once (up to 64), four planes per 16-byte
+// shared store (a quarter warp's stores, VP words per slot apart, fill
+// distinct bank groups).  For FP32 input this takes the P = 3 step from 5.60
+// to 5.41 ms against 4-byte asynchronous copies (one slot per thread put 4
+// lanes on every bank; 8 slots x 4 planes per warp instruction is
+// conflict-free but makes four dependent passes per warp: 5.87 ms), and 16
+// loads per batch instead of 8 another 0.05 ms.  The caller synchronises
+// after it.
+template <int P, typename TIn, int MTY, int NTHREAD>
+__device__ __forceinline__ void gather_tile(const MixArgs& a, int j0, int i0, float* sd, uint8_t* sk, int tid) {
+    constexpr int NQ = P + 1, NM = NQ * NQ, VP = vpitch(NM), SD = SX * (MTY + 2);
+    const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
+    const size_t plane = a.g.plane;
+    for (int slot = tid; slot < SD; slot += NTHREAD) {
+        const int r = slot / SX, c = slot - r * SX;
+        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
+        uint8_t kd = KIND_PASSIVE;
+        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+            const size_t k = (size_t)gi * pitch + gj;
+            kd = a.kind[k] & KIND_MASK;
+            size_t ks = k;
+            int neg = -1;
+            if (kd >= KIND_COPY) {
+                ks = (size_t)a.gsrc[k];
+                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
+            }
+#pragma unroll 16
+            for (int v = 0; v < 4 * NM; v += 4) {
+                float4 x;
+                x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
+                x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
+                x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
+                x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
+                if (neg == (v + 0) / NM) x.x = -x.x;
+                if (neg == (v + 1) / NM) x.y = -x.y;
+                if (neg == (v + 2) / NM) x.z = -x.z;
+                if (neg == (v + 3) / NM) x.w = -x.w;
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
+            }
+        } else {
+            for (int v = 0; v < 4 * NM; v += 4)
+                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        sk[slot] = kd;
+    }
+}
+
 // One tile whose top-left cell is (i0, j0), shared memory at `smem`
 // (smem_bytes<P, MTY>()).  Per-thread returns leave only this function: every
 // barrier of the tile precedes them.  LAM (FP64 output only): returns the max
@@ -387,52 +438,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     }
 
     // 0. gather tile + halo (corners unused)
-    for (int slot = tid; slot < SD; slot += MNT) {
-        const int r = slot / SX, c = slot - r * SX;
-        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        uint8_t kd = KIND_PASSIVE;
-        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
-            const size_t k = (size_t)gi * pitch + gj;
-            kd = a.kind[k] & KIND_MASK;
-            size_t ks = k;
-            int neg = -1;
-            if (kd >= KIND_COPY) {
-                ks = (size_t)a.gsrc[k];
-                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
-            }
-            if (sizeof(TIn) == 4) {
-                // FP32 input: asynchronous 4-byte copies, all in flight at once
-                const float* src = static_cast<const float*>(a.cur) + ks;
-#pragma unroll 8
-                for (int v = 0; v < 4 * NM; ++v) {
-                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
-                                 : "memory");
-                }
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                if (neg >= 0)
-                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
-            } else {
-#pragma unroll 8
-                for (int v = 0; v < 4 * NM; v += 4) {
-                    float4 x;
-                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
-                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
-                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
-                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
-                    if (neg == (v + 0) / NM) x.x = -x.x;
-                    if (neg == (v + 1) / NM) x.y = -x.y;
-                    if (neg == (v + 2) / NM) x.z = -x.z;
-                    if (neg == (v + 3) / NM) x.w = -x.w;
-                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
-                }
-            }
-        } else {
-            for (int v = 0; v < 4 * NM; v += 4)
-                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        sk[slot] = kd;
-    }
+    gather_tile<P, TIn, MTY, MNT>(a, j0, i0, sd, sk, tid);
     __syncthreads();
 
     // 1. interface fluxes of the tile, once each
@@ -765,6 +771,16 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     return umax;
 }
 
+// Lanes of a cell in the two-threads-per-cell kernels: lane l (bit 3 clear)
+// holds half 0 and lane l + 8 half 1 of the warp's cell (l >> 4) * 8 + (l & 7).
+// Eight consecutive lanes thus read one half of 8 consecutive cells, whose
+// slots lie VP words apart: their float4 loads fall in 8 distinct bank groups
+// (with the partners one lane apart, both halves of a cell, 2 NM words apart,
+// shared their banks: every volume load was a 2-way conflict).
+constexpr int kPairLane = 8;
+__device__ __forceinline__ int pair_half(int t) { return (t >> 3) & 1; }
+__device__ __forceinline__ int pair_cell(int t) { return ((t >> 4) << 3) | (t & 7); }
+
 // Shared memory of the fused indicator: one [16][MLP_TILE_KP] BF16 feature
 // tile per warp (8 warps).  It reuses the interface-flux region, free once
 // every cell has taken its face integrals, where that region is large enough
@@ -803,7 +819,7 @@ __device__ __forceinline__ void indicator_epilogue(const MixArgs& a, const float
                                                    size_t k) {
     constexpr int NQ = P + 1, NM = NQ * NQ, VP = vpitch(NM);
     constexpr unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31, row = lane >> 1;
+    const int lane = threadIdx.x & 31, row = pair_cell(lane);
     float f[20];
 #pragma unroll
     for (int i = 0; i < 20; ++i) f[i] = 0.0f;
@@ -827,7 +843,7 @@ __device__ __forceinline__ void indicator_epilogue(const MixArgs& a, const float
 #pragma unroll
         for (int i = 0; i < 20; ++i) dev = fmaxf(dev, fabsf(f[i]));
     }
-    dev = fmaxf(dev, __shfl_xor_sync(FULL, dev, 1));
+    dev = fmaxf(dev, __shfl_xor_sync(FULL, dev, kPairLane));
     const bool cand = upd && !(dev <= a.screen);
     __syncthreads();  // every face integral is taken: the flux region may hold the feature tiles
     const bool warp_runs = __any_sync(FULL, cand);
@@ -927,7 +943,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);
     uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);
 
-    const int tid = threadIdx.x, h = tid & 1, ci = tid >> 1;
+    const int tid = threadIdx.x, h = pair_half(tid), ci = pair_cell(tid);
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
 
@@ -942,52 +958,8 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         }
     }
 
-    // 0. gather tile + halo (as stage_tile, over all NT threads)
-    for (int slot = tid; slot < SD; slot += NT) {
-        const int r = slot / SX, c = slot - r * SX;
-        const int gi = i0 - 1 + r, gj = j0 - 1 + c;
-        uint8_t kd = KIND_PASSIVE;
-        if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
-            const size_t k = (size_t)gi * pitch + gj;
-            kd = a.kind[k] & KIND_MASK;
-            size_t ks = k;
-            int neg = -1;
-            if (kd >= KIND_COPY) {
-                ks = (size_t)a.gsrc[k];
-                neg = (kd == KIND_SLIP_X) ? 1 : (kd == KIND_SLIP_Y ? 2 : -1);
-            }
-            if (sizeof(TIn) == 4) {
-                const float* src = static_cast<const float*>(a.cur) + ks;
-#pragma unroll 8
-                for (int v = 0; v < 4 * NM; ++v) {
-                    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&sd[slot * VP + v]);
-                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + (size_t)v * plane)
-                                 : "memory");
-                }
-                asm volatile("cp.async.wait_all;" ::: "memory");
-                if (neg >= 0)
-                    for (int m = 0; m < NM; ++m) sd[slot * VP + neg * NM + m] = -sd[slot * VP + neg * NM + m];
-            } else {
-#pragma unroll 8
-                for (int v = 0; v < 4 * NM; v += 4) {
-                    float4 x;
-                    x.x = load_f<TIn>(a.cur, (size_t)(v + 0) * plane + ks);
-                    x.y = load_f<TIn>(a.cur, (size_t)(v + 1) * plane + ks);
-                    x.z = load_f<TIn>(a.cur, (size_t)(v + 2) * plane + ks);
-                    x.w = load_f<TIn>(a.cur, (size_t)(v + 3) * plane + ks);
-                    if (neg == (v + 0) / NM) x.x = -x.x;
-                    if (neg == (v + 1) / NM) x.y = -x.y;
-                    if (neg == (v + 2) / NM) x.z = -x.z;
-                    if (neg == (v + 3) / NM) x.w = -x.w;
-                    *reinterpret_cast<float4*>(&sd[slot * VP + v]) = x;
-                }
-            }
-        } else {
-            for (int v = 0; v < 4 * NM; v += 4)
-                *reinterpret_cast<float4*>(&sd[slot * VP + v]) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        sk[slot] = kd;
-    }
+    // 0. gather tile + halo over all NT threads
+    gather_tile<P, TIn, MTY, NT>(a, j0, i0, sd, sk, tid);
     __syncthreads();
 
     // 1. interface fluxes: one thread per face (all four variables), so no
@@ -1045,7 +1017,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                     uo[cc] = x;
                 }
                 float U[4];
-                join_pair(h, uo[0], uo[1], __shfl_xor_sync(um, uo[0], 1), __shfl_xor_sync(um, uo[1], 1), U);
+                join_pair(h, uo[0], uo[1], __shfl_xor_sync(um, uo[0], kPairLane), __shfl_xor_sync(um, uo[1], kPairLane), U);
                 float F[4], G[4];
                 euler_flux_f(U, a.gamma, F, G);
                 const float w = S.W[qa] * S.W[qb];
@@ -1191,7 +1163,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         }
         const float RHO_MIN = 1e-5f, P_MIN = 1e-5f, EPS = 1e-5f, g1 = a.gamma - 1.0f;
         float m0[4];  // the cell means of all four variables
-        join_pair(h, acc[0][0], acc[1][0], __shfl_xor_sync(lm, acc[0][0], 1), __shfl_xor_sync(lm, acc[1][0], 1), m0);
+        join_pair(h, acc[0][0], acc[1][0], __shfl_xor_sync(lm, acc[0][0], kPairLane), __shfl_xor_sync(lm, acc[1][0], kPairLane), m0);
         if (m0[0] < RHO_MIN) { m0[0] = RHO_MIN; rho_clamp = true; }
         const float rho0 = m0[0], mx0 = m0[1], my0 = m0[2];
         const float ke0 = half_m2_over_rho(rho0, mx0, my0);
@@ -1204,7 +1176,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         float th = 1.0f;
         float spo[2] = {zs_spread<P, NM>(acc[0]), zs_spread<P, NM>(acc[1])};  // this half's spreads
         float sp[4];
-        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], 1), __shfl_xor_sync(lm, spo[1], 1), sp);
+        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], kPairLane), __shfl_xor_sync(lm, spo[1], kPairLane), sp);
         const bool rho_pass = !zs_above(rho0, sp[0], RHO_MIN);  // the same decision in both halves
 #pragma unroll 1
         for (int za = 0; za < (rho_pass ? 4 : 0); ++za) {
@@ -1225,7 +1197,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             }
         }
         {
-            const float tho = __shfl_xor_sync(lm, th, 1);
+            const float tho = __shfl_xor_sync(lm, th, kPairLane);
             th = h ? tho : th;
         }
         if (th < 1.0f) {
@@ -1239,7 +1211,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
         // the spreads after the density factor (every lane of lm shuffles)
         spo[0] = zs_spread<P, NM>(acc[0]);
         spo[1] = zs_spread<P, NM>(acc[1]);
-        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], 1), __shfl_xor_sync(lm, spo[1], 1), sp);
+        join_pair(h, spo[0], spo[1], __shfl_xor_sync(lm, spo[0], kPairLane), __shfl_xor_sync(lm, spo[1], kPairLane), sp);
         const bool p_pass = !zs_p_above(m0, sp, g1, RHO_MIN, P_MIN);  // the same in both halves
         const unsigned zm = __ballot_sync(lm, p_pass);                 // lanes that run the pressure pass
 #pragma unroll 1
@@ -1265,7 +1237,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
                     uo[cc] = x;
                 }
                 float U[4];
-                join_pair(h, uo[0], uo[1], __shfl_xor_sync(zm, uo[0], 1), __shfl_xor_sync(zm, uo[1], 1), U);
+                join_pair(h, uo[0], uo[1], __shfl_xor_sync(zm, uo[0], kPairLane), __shfl_xor_sync(zm, uo[1], kPairLane), U);
                 if (U[0] <= RHO_MIN) continue;
                 const float p = pressure_f(g1, U[0], U[1], U[2], U[3]);
                 if (p < P_MIN) tp = fminr(tp, zs_ratio(p_avg, P_MIN, p, EPS));
@@ -1333,7 +1305,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             double full[4][4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const double o0 = __shfl_xor_sync(pm, cs[e][0], 1), o1 = __shfl_xor_sync(pm, cs[e][1], 1);
+                const double o0 = __shfl_xor_sync(pm, cs[e][0], kPairLane), o1 = __shfl_xor_sync(pm, cs[e][1], kPairLane);
                 full[e][0] = h ? o0 : cs[e][0];
                 full[e][1] = h ? o1 : cs[e][1];
                 full[e][2] = h ? cs[e][0] : o0;
@@ -1341,7 +1313,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             }
             if (a.kind[k] & KIND_FLUID) umax = dg_cell_speed(full, a.gamma64, 0.0);
         }
-        const double p0 = __shfl_xor_sync(pm, om[0], 1), p1 = __shfl_xor_sync(pm, om[1], 1);
+        const double p0 = __shfl_xor_sync(pm, om[0], kPairLane), p1 = __shfl_xor_sync(pm, om[1], kPairLane);
         if (kd == KIND_UPDATED && h == 0) {
             const double rho = om[0], mx = om[1], my = p0, E = p1;
             const double p = (double)(a.gamma - 1.0f) * (E - 0.5 * (mx * mx + my * my) / rho);
