@@ -243,6 +243,16 @@ __device__ __forceinline__ bool zs_p_above(const float (&mean)[4], const float (
 // odd, which puts 8 consecutive cells' 16-byte loads in 8 distinct bank groups.
 __host__ __device__ constexpr int vpitch(int nm) { return ((4 * nm / 4) % 2 == 1) ? 4 * nm : 4 * nm + 4; }
 
+// Plane strides (words) of the interface-flux arrays: x faces MTY rows of
+// MTX + 1, y faces MTY + 1 rows of MTX, each padded to 8 (mod 16).  In the
+// two-threads-per-cell face integrals a warp reads one plane per half, 2
+// planes apart, for 16 consecutive cells: offsets 0, 8 (cells 8-15) and
+// 2 stride, 2 stride + 8 (the other half) then fall on 4 distinct groups of 8
+// banks (unpadded, 132 and 160 words, two groups shared their banks).
+__host__ __device__ constexpr int pad8mod16(int n) { return n + ((8 - n % 16) + 16) % 16; }
+__host__ __device__ constexpr int fx_stride(int mty) { return pad8mod16(mty * (MTX + 1)); }
+__host__ __device__ constexpr int fy_stride(int mty) { return pad8mod16((mty + 1) * MTX); }
+
 template <typename T>
 __device__ __forceinline__ float load_f(const void* p, size_t i) {
     return (float)static_cast<const T*>(p)[i];
@@ -270,7 +280,7 @@ __device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* 
             sr = sl + 1;                     // right cell slot
             side_l = 0; side_r = 1;          // xi=+1 of left, xi=-1 of right
             dst = sfx + r * (MTX + 1) + c;
-            dstride = MTY * (MTX + 1);
+            dstride = fx_stride(MTY);
             ydir = false;
         } else {
             const int g = f - NXF, r = g / MTX, c = g - r * MTX;
@@ -278,7 +288,7 @@ __device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* 
             sr = sl + SX;                    // cell below
             side_l = 2; side_r = 3;          // eta=+1 of upper, eta=-1 of lower
             dst = sfy + r * MTX + c;
-            dstride = (MTY + 1) * MTX;
+            dstride = fy_stride(MTY);
             ydir = true;
         }
         if (sk[sl] != KIND_UPDATED && sk[sr] != KIND_UPDATED) continue;
@@ -418,8 +428,8 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
     const DGSepF& S = c_sepf[P - 1];
     float* sd = smem;                       // [SD][VP] gathered stage input, cell-major
     float* sfx = sd + VP * SD;              // [NQ*4][MTY][MTX+1]
-    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);  // [NQ*4][MTY+1][MTX]
-    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);  // [SY][SX]
+    float* sfy = sfx + NQ * 4 * fx_stride(MTY);  // [NQ*4][MTY+1][MTX] at fy_stride per plane
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * fy_stride(MTY));  // [SY][SX]
 
     const int tid = threadIdx.x;
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
@@ -532,7 +542,7 @@ __device__ __forceinline__ double stage_tile(const MixArgs& a, int j0, int i0, f
             const float* Fl = sfx + r * (MTX + 1) + c;
             const float* Fd = sfy + (r + 1) * MTX + c;
             const float* Fu = sfy + r * MTX + c;
-            constexpr int fsx = MTY * (MTX + 1), fsy = (MTY + 1) * MTX;
+            constexpr int fsx = fx_stride(MTY), fsy = fy_stride(MTY);
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 float hr[NQ], hl[NQ], hd[NQ], hu[NQ];
@@ -791,7 +801,7 @@ constexpr size_t kMlpTileBytes = 8 * 16 * MLP_TILE_KP * sizeof(uint16_t);
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
 template <int P, int MTY>
 constexpr bool mlp_tiles_in_flux() {
-    return sizeof(float) * (P + 1) * 4 * (MTY * (MTX + 1) + (MTY + 1) * MTX) >= kMlpTileBytes;
+    return sizeof(float) * (P + 1) * 4 * (fx_stride(MTY) + fy_stride(MTY)) >= kMlpTileBytes;
 }
 
 // Round-to-nearest BF16 pair, lo in the low half.
@@ -940,8 +950,8 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     const DGSepF& S = c_sepf[P - 1];
     float* sd = smem;
     float* sfx = sd + VP * SD;
-    float* sfy = sfx + NQ * 4 * MTY * (MTX + 1);
-    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * (MTY + 1) * MTX);
+    float* sfy = sfx + NQ * 4 * fx_stride(MTY);
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * fy_stride(MTY));
 
     const int tid = threadIdx.x, h = pair_half(tid), ci = pair_cell(tid);
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
@@ -1056,7 +1066,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
             const float* Fl = sfx + r * (MTX + 1) + c;
             const float* Fd = sfy + (r + 1) * MTX + c;
             const float* Fu = sfy + r * MTX + c;
-            constexpr int fsx = MTY * (MTX + 1), fsy = (MTY + 1) * MTX;
+            constexpr int fsx = fx_stride(MTY), fsy = fy_stride(MTY);
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int u = 2 * h + cc;
@@ -1326,7 +1336,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     const double umax_cell = cell_phase();
     if constexpr (MLP) {
         // feature tiles: the flux region, or after the stage's shared memory
-        constexpr size_t own = sizeof(float) * (VP * SD + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SD;
+        constexpr size_t own = sizeof(float) * (VP * SD + NQ * 4 * fx_stride(MTY) + NQ * 4 * fy_stride(MTY)) + SD;
         uint16_t* tiles = mlp_tiles_in_flux<P, MTY>() ? reinterpret_cast<uint16_t*>(sfx)
                                                      : reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(smem) +
                                                                                    align16(own));
@@ -1338,7 +1348,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
 template <int P, int MTY>
 constexpr size_t smem_bytes() {
     constexpr int NQ = P + 1, NM = NQ * NQ, SY = MTY + 2;
-    return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * MTY * (MTX + 1) + NQ * 4 * (MTY + 1) * MTX) + SX * SY;
+    return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * fx_stride(MTY) + NQ * 4 * fy_stride(MTY)) + SX * SY;
 }
 
 // resident CTAs per SM: 8 for P=1 (+5% over 3), 3 for P=2 (4 and 5 were
