@@ -250,8 +250,8 @@ __host__ __device__ constexpr int vpitch(int nm) { return ((4 * nm / 4) % 2 == 1
 // 2 stride, 2 stride + 8 (the other half) then fall on 4 distinct groups of 8
 // banks (unpadded, 132 and 160 words, two groups shared their banks).
 __host__ __device__ constexpr int pad8mod16(int n) { return n + ((8 - n % 16) + 16) % 16; }
-__host__ __device__ constexpr int fx_stride(int mty) { return pad8mod16(mty * (MTX + 1)); }
-__host__ __device__ constexpr int fy_stride(int mty) { return pad8mod16((mty + 1) * MTX); }
+__host__ __device__ constexpr int fx_stride(int mty, int tx = MTX) { return pad8mod16(mty * (tx + 1)); }
+__host__ __device__ constexpr int fy_stride(int mty, int tx = MTX) { return pad8mod16((mty + 1) * tx); }
 
 template <typename T>
 __device__ __forceinline__ float load_f(const void* p, size_t i) {
@@ -262,33 +262,33 @@ __device__ __forceinline__ float load_f(const void* p, size_t i) {
 // shared memory): faces dealt to the NTHREAD threads in turn, each thread the
 // whole face (all four variables).  Shared by the one- and two-thread-per-cell
 // stages.
-template <int P, int MTY, int NTHREAD>
+template <int P, int MTY, int NTHREAD, int TX = MTX>
 __device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* sd, float* sfx, float* sfy,
                                                  const uint8_t* sk, int tid) {
     constexpr int NQ = P + 1, NM = NQ * NQ;
     constexpr int VP = vpitch(NM);
     const DGSepF& S = c_sepf[P - 1];
-    constexpr int NXF = MTY * (MTX + 1), NYF = (MTY + 1) * MTX;
+    constexpr int SXT = TX + 2, NXF = MTY * (TX + 1), NYF = (MTY + 1) * TX;
     for (int f = tid; f < NXF + NYF; f += NTHREAD) {
         int sl, sr, side_l, side_r;
         float* dst;
         int dstride;
         bool ydir;
         if (f < NXF) {
-            const int r = f / (MTX + 1), c = f - r * (MTX + 1);
-            sl = (r + 1) * SX + c;          // left cell slot
+            const int r = f / (TX + 1), c = f - r * (TX + 1);
+            sl = (r + 1) * SXT + c;          // left cell slot
             sr = sl + 1;                     // right cell slot
             side_l = 0; side_r = 1;          // xi=+1 of left, xi=-1 of right
-            dst = sfx + r * (MTX + 1) + c;
-            dstride = fx_stride(MTY);
+            dst = sfx + r * (TX + 1) + c;
+            dstride = fx_stride(MTY, TX);
             ydir = false;
         } else {
-            const int g = f - NXF, r = g / MTX, c = g - r * MTX;
-            sl = r * SX + c + 1;             // cell above
-            sr = sl + SX;                    // cell below
+            const int g = f - NXF, r = g / TX, c = g - r * TX;
+            sl = r * SXT + c + 1;             // cell above
+            sr = sl + SXT;                    // cell below
             side_l = 2; side_r = 3;          // eta=+1 of upper, eta=-1 of lower
-            dst = sfy + r * MTX + c;
-            dstride = fy_stride(MTY);
+            dst = sfy + r * TX + c;
+            dstride = fy_stride(MTY, TX);
             ydir = true;
         }
         if (sk[sl] != KIND_UPDATED && sk[sr] != KIND_UPDATED) continue;
@@ -375,13 +375,13 @@ __device__ __forceinline__ void tile_face_fluxes(const MixArgs& a, const float* 
 // conflict-free but makes four dependent passes per warp: 5.87 ms), and 16
 // loads per batch instead of 8 another 0.05 ms.  The caller synchronises
 // after it.
-template <int P, typename TIn, int MTY, int NTHREAD>
+template <int P, typename TIn, int MTY, int NTHREAD, int TX = MTX>
 __device__ __forceinline__ void gather_tile(const MixArgs& a, int j0, int i0, float* sd, uint8_t* sk, int tid) {
-    constexpr int NQ = P + 1, NM = NQ * NQ, VP = vpitch(NM), SD = SX * (MTY + 2);
+    constexpr int SXT = TX + 2, NQ = P + 1, NM = NQ * NQ, VP = vpitch(NM), SD = SXT * (MTY + 2);
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
     const size_t plane = a.g.plane;
     for (int slot = tid; slot < SD; slot += NTHREAD) {
-        const int r = slot / SX, c = slot - r * SX;
+        const int r = slot / SXT, c = slot - r * SXT;
         const int gi = i0 - 1 + r, gj = j0 - 1 + c;
         uint8_t kd = KIND_PASSIVE;
         if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
@@ -799,9 +799,9 @@ __device__ __forceinline__ int pair_cell(int t) { return ((t >> 4) << 3) | (t & 
 // stage: measured slower).
 constexpr size_t kMlpTileBytes = 8 * 16 * MLP_TILE_KP * sizeof(uint16_t);
 __host__ __device__ constexpr size_t align16(size_t n) { return (n + 15) & ~size_t(15); }
-template <int P, int MTY>
+template <int P, int MTY, int TX = MTX>
 constexpr bool mlp_tiles_in_flux() {
-    return sizeof(float) * (P + 1) * 4 * (fx_stride(MTY) + fy_stride(MTY)) >= kMlpTileBytes;
+    return sizeof(float) * (P + 1) * 4 * (fx_stride(MTY, TX) + fy_stride(MTY, TX)) >= kMlpTileBytes;
 }
 
 // Round-to-nearest BF16 pair, lo in the low half.
@@ -823,7 +823,7 @@ __device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
 // cells go through the MLP on the tensor cores (mlp_logits16), and half 0 of
 // every updated, unscreened cell with a positive logit appends the cell to the
 // list, which the TVB list pass then limits.
-template <int P>
+template <int P, int TX = MTX>
 __device__ __forceinline__ void indicator_epilogue(const MixArgs& a, const float* sd, uint16_t* ftiles, int slot,
                                                    int h, bool upd, const float (&acc)[2][(P + 1) * (P + 1)],
                                                    size_t k) {
@@ -838,7 +838,7 @@ __device__ __forceinline__ void indicator_epilogue(const MixArgs& a, const float
         const int var = h ? 3 : 0;
         const float m0 = sd[slot * VP + var * NM];
         const float mL = sd[(slot - 1) * VP + var * NM], mR = sd[(slot + 1) * VP + var * NM];
-        const float mU = sd[(slot - SX) * VP + var * NM], mD = sd[(slot + SX) * VP + var * NM];
+        const float mU = sd[(slot - (TX + 2)) * VP + var * NM], mD = sd[(slot + (TX + 2)) * VP + var * NM];
         const float sc = fmaxf(fmaxf(fmaxf(fabsf(m0), fabsf(mL)), fmaxf(fabsf(mR), fabsf(mU))), fabsf(mD)) + 1e-12f;
         const float is = 1.0f / sc;
 #pragma unroll
@@ -939,19 +939,19 @@ __device__ __forceinline__ void join_pair(int h, float a0, float a1, float o0, f
 // bits.  Shuffles run under masks taken by ballot over lanes that are all
 // present: the face loop has a warp-uniform trip count and the cell phase
 // returns only after its last shuffle.
-template <int P, typename TIn, typename TOut, int MTY, bool LAM = false, bool MLP = false>
+template <int P, typename TIn, typename TOut, int MTY, bool LAM = false, bool MLP = false, int TX = MTX>
 __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int i0, float* smem) {
-    constexpr int MNT = MTX * MTY, NT = 2 * MNT, SY = MTY + 2;
+    constexpr int SXT = TX + 2, MNT = TX * MTY, NT = 2 * MNT, SY = MTY + 2;
     constexpr int NQ = P + 1, NM = NQ * NQ;
-    constexpr int SD = SX * SY;
+    constexpr int SD = SXT * SY;
     constexpr int VP = vpitch(NM);
     constexpr int VW = HalfVec<NM>::VW;
     constexpr unsigned FULL = 0xffffffffu;
     const DGSepF& S = c_sepf[P - 1];
     float* sd = smem;
     float* sfx = sd + VP * SD;
-    float* sfy = sfx + NQ * 4 * fx_stride(MTY);
-    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * fy_stride(MTY));
+    float* sfy = sfx + NQ * 4 * fx_stride(MTY, TX);
+    uint8_t* sk = reinterpret_cast<uint8_t*>(sfy + NQ * 4 * fy_stride(MTY, TX));
 
     const int tid = threadIdx.x, h = pair_half(tid), ci = pair_cell(tid);
     const int ny = a.g.ny, nx = a.g.nx, pitch = a.g.pitch;
@@ -959,7 +959,7 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
 
     // U^n of this half's variables, towards L2 (read again only by the combine)
     {
-        const int pr = ci / MTX, pc = ci - pr * MTX;
+        const int pr = ci / TX, pc = ci - pr * TX;
         if (i0 + pr < ny && j0 + pc < nx) {
             const double* u0 = a.un + (size_t)(2 * h * NM) * plane + (size_t)(i0 + pr) * pitch + (j0 + pc);
 #pragma unroll 8
@@ -969,21 +969,21 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     }
 
     // 0. gather tile + halo over all NT threads
-    gather_tile<P, TIn, MTY, NT>(a, j0, i0, sd, sk, tid);
+    gather_tile<P, TIn, MTY, NT, TX>(a, j0, i0, sd, sk, tid);
     __syncthreads();
 
     // 1. interface fluxes: one thread per face (all four variables), so no
     //    flux is evaluated twice and the 256 threads cover the faces in two rounds
-    tile_face_fluxes<P, MTY, NT>(a, sd, sfx, sfy, sk, tid);
+    tile_face_fluxes<P, MTY, NT, TX>(a, sd, sfx, sfy, sk, tid);
     // no barrier yet: the volume quadrature reads only the gathered state, so
     // warps without a second face start on it while the last faces finish
 
     // 2. one lane pair per cell
-    const int r = ci / MTX, c = ci - r * MTX;
+    const int r = ci / TX, c = ci - r * TX;
     const int gi = i0 + r, gj = j0 + c;
     const bool inside = gi < ny && gj < nx;
     const unsigned pm = __ballot_sync(FULL, inside);  // lanes of cells in the grid (whole pairs)
-    const int slot = (r + 1) * SX + c + 1;
+    const int slot = (r + 1) * SXT + c + 1;
     const size_t k = inside ? (size_t)gi * pitch + gj : 0;
     const uint8_t kd = inside ? sk[slot] : (uint8_t)KIND_PASSIVE;
     const unsigned um = __ballot_sync(FULL, kd == KIND_UPDATED);
@@ -1062,11 +1062,11 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     if (kd == KIND_UPDATED) {
         // face integrals of this half's variables (order of stage_tile)
         {
-            const float* Fr = sfx + r * (MTX + 1) + c + 1;
-            const float* Fl = sfx + r * (MTX + 1) + c;
-            const float* Fd = sfy + (r + 1) * MTX + c;
-            const float* Fu = sfy + r * MTX + c;
-            constexpr int fsx = fx_stride(MTY), fsy = fy_stride(MTY);
+            const float* Fr = sfx + r * (TX + 1) + c + 1;
+            const float* Fl = sfx + r * (TX + 1) + c;
+            const float* Fd = sfy + (r + 1) * TX + c;
+            const float* Fu = sfy + r * TX + c;
+            constexpr int fsx = fx_stride(MTY, TX), fsy = fy_stride(MTY, TX);
 #pragma unroll
             for (int cc = 0; cc < 2; ++cc) {
                 const int u = 2 * h + cc;
@@ -1336,19 +1336,20 @@ __device__ __forceinline__ double stage_tile_pair(const MixArgs& a, int j0, int 
     const double umax_cell = cell_phase();
     if constexpr (MLP) {
         // feature tiles: the flux region, or after the stage's shared memory
-        constexpr size_t own = sizeof(float) * (VP * SD + NQ * 4 * fx_stride(MTY) + NQ * 4 * fy_stride(MTY)) + SD;
-        uint16_t* tiles = mlp_tiles_in_flux<P, MTY>() ? reinterpret_cast<uint16_t*>(sfx)
+        constexpr size_t own = sizeof(float) * (VP * SD + NQ * 4 * fx_stride(MTY, TX) + NQ * 4 * fy_stride(MTY, TX)) + SD;
+        uint16_t* tiles = mlp_tiles_in_flux<P, MTY, TX>() ? reinterpret_cast<uint16_t*>(sfx)
                                                      : reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(smem) +
                                                                                    align16(own));
-        if (a.stage > 0) indicator_epilogue<P>(a, sd, tiles, slot, h, inside && kd == KIND_UPDATED, acc, k);
+        if (a.stage > 0) indicator_epilogue<P, TX>(a, sd, tiles, slot, h, inside && kd == KIND_UPDATED, acc, k);
     }
     return umax_cell;
 }
 
-template <int P, int MTY>
+template <int P, int MTY, int TX = MTX>
 constexpr size_t smem_bytes() {
-    constexpr int NQ = P + 1, NM = NQ * NQ, SY = MTY + 2;
-    return sizeof(float) * (vpitch(NM) * SX * SY + NQ * 4 * fx_stride(MTY) + NQ * 4 * fy_stride(MTY)) + SX * SY;
+    constexpr int NQ = P + 1, NM = NQ * NQ, SY = MTY + 2, SXT = TX + 2;
+    return sizeof(float) * (vpitch(NM) * SXT * SY + NQ * 4 * fx_stride(MTY, TX) + NQ * 4 * fy_stride(MTY, TX)) +
+           SXT * SY;
 }
 
 // resident CTAs per SM: 8 for P=1 (+5% over 3), 3 for P=2 (4 and 5 were
@@ -1364,25 +1365,31 @@ __global__ void __launch_bounds__(MTX * 4, P == 1 ? 8 : 3) dg_stage_mixed_kernel
 // spills; 512 ran 15% slower), 512 for P = 3 (2 CTAs of 8 warps at 128
 // registers; 768 spilled and ran 17% slower).
 constexpr int pair_thread_budget(int P) { return P == 1 ? 1024 : P == 3 ? 512 : 768; }
-// Tile rows of the single-problem two-threads-per-cell kernel: 32 x 2 tiles (4
-// CTAs of 128 threads, the same 16 warps per SM) ran 9% slower at P = 3 (the
-// 1-cell halo is 2.1x the tile's cells instead of 1.6x).
-constexpr int kPairRows = 4;
+// Tile of the single-problem two-threads-per-cell kernel (columns x rows).
+// 16 x 8 gathers 1.41 halo slots per cell and leaves 24 of its 280 faces for
+// a second round of the 256 threads; 32 x 4: 1.59 and 36 of 292.  P = 3 step
+// with the fused indicator at 2048^2: 5.355 vs 5.394 ms, P = 2 2.605 vs 2.656
+// ms (P = 3 with the reference limiter 5.237 vs 5.199).  32 x 2 (4 CTAs of
+// 128 threads, the same 16 warps per SM, halo 2.1x) ran 9% slower than 32 x 4.
+constexpr int kPairCols = 16, kPairRows = 8;
 // Shared memory of the single-problem pair kernel, with the indicator's
 // feature tiles when MLP.
 template <int P, bool MLP>
 constexpr size_t pair_smem_bytes() {
-    return MLP && !mlp_tiles_in_flux<P, kPairRows>() ? align16(smem_bytes<P, kPairRows>()) + kMlpTileBytes
-                                                    : smem_bytes<P, kPairRows>();
+    return MLP && !mlp_tiles_in_flux<P, kPairRows, kPairCols>()
+               ? align16(smem_bytes<P, kPairRows, kPairCols>()) + kMlpTileBytes
+               : smem_bytes<P, kPairRows, kPairCols>();
 }
 template <int P, bool MLP = false>
 constexpr int pair_min_blocks() {
-    return batch_min_blocks(MTX * 2 * kPairRows, pair_thread_budget(P), pair_smem_bytes<P, MLP>());
+    return batch_min_blocks(kPairCols * 2 * kPairRows, pair_thread_budget(P), pair_smem_bytes<P, MLP>());
 }
 template <int P, typename TIn, typename TOut, bool MLP>
-__global__ void __launch_bounds__(MTX * 2 * kPairRows, pair_min_blocks<P, MLP>()) dg_stage_mixed_pair_kernel(MixArgs a) {
+__global__ void __launch_bounds__(kPairCols * 2 * kPairRows, pair_min_blocks<P, MLP>())
+    dg_stage_mixed_pair_kernel(MixArgs a) {
     extern __shared__ __align__(16) float smem[];
-    stage_tile_pair<P, TIn, TOut, kPairRows, false, MLP>(a, blockIdx.x * MTX, blockIdx.y * kPairRows, smem);
+    stage_tile_pair<P, TIn, TOut, kPairRows, false, MLP, kPairCols>(a, blockIdx.x * kPairCols, blockIdx.y * kPairRows,
+                                                                    smem);
 }
 
 // Default threads per cell of the single-problem stage kernel, per P, when
@@ -1488,7 +1495,7 @@ template <int P, typename TIn, typename TOut, int TPC, bool MLP>
 cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
     constexpr bool pair = TPC == 2;
     static_assert(pair || !MLP, "the fused indicator runs in the two-threads-per-cell kernel");
-    constexpr int rows = pair ? kPairRows : 4;
+    constexpr int rows = pair ? kPairRows : 4, cols = pair ? kPairCols : MTX;
     constexpr size_t sm = pair ? pair_smem_bytes<P, MLP>() : smem_bytes<P, rows>();
     auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut, MLP> : dg_stage_mixed_kernel<P, TIn, TOut>;
     static bool attr_set[64] = {};
@@ -1499,8 +1506,8 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
         if (e != cudaSuccess) return e;
         attr_set[dev] = true;
     }
-    dim3 grid((a.g.nx + MTX - 1) / MTX, (a.g.ny + rows - 1) / rows);
-    kern<<<grid, MTX * rows * TPC, sm, s>>>(a);
+    dim3 grid((a.g.nx + cols - 1) / cols, (a.g.ny + rows - 1) / rows);
+    kern<<<grid, cols * rows * TPC, sm, s>>>(a);
     return cudaGetLastError();
 }
 
