@@ -54,9 +54,13 @@ FLOPS_PER_CELL_STAGE = {("weno", 0): WENO_FLOPS_PER_CELL_STAGE, ("dg", 1): 1700.
 # cells; None where not captured.  Keyed by (workload, precision):
 # (bytes per updated cell, what was captured).
 KERNEL_TRAFFIC_PER_CELL: dict = {
-    ("dg3_fq_2048", "mixed"): (977.2, "dg_stage_mixed_pair_kernel<3,float,float,MLP> (stage 2) at 512^2: "
-                                      "201.8 MB read + 48.3 MB written"),
+    ("dg3_fq_2048", "mixed", "dg_stage_mixed_pair_kernel"): (
+        977.2, "dg_stage_mixed_pair_kernel<3,float,float,MLP> (stage 2) at 512^2: 201.8 MB read + 48.3 MB written"),
+    ("weno_fq_2048", "mixed", "weno_stage_mixed_kernel"): (
+        57.7, "weno_stage_mixed_kernel (stage 1) at 2048^2: 139.2 MB read + 101.4 MB written"),
 }
+# the mixed DG stage kernel for each threads-per-cell choice of the tuner
+DG_MIXED_KERNEL = {1: "dg_stage_mixed_kernel", 2: "dg_stage_mixed_pair_kernel", 4: "dg_stage_mixed_quad_kernel"}
 
 
 def make_workload(name: str, rank: int):
@@ -330,7 +334,8 @@ def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: 
         barrier(pg)
         ms_max = allreduce_max(pg, ms)
         paths[prec] = {"ms": ms, "ms_max": ms_max, "status": s.status_word(), "clocks": clk.summary(),
-                       "value": world * dofs * args.steps / (ms_max * 1e-3), "solver": s}
+                       "value": world * dofs * args.steps / (ms_max * 1e-3), "solver": s,
+                       "tpc": s.tile_tpc() if (w["method"] == "dg" and prec == "mixed") else None}
     head = "mixed" if "mixed" in paths else "fp64"
     hp = paths[head]
     # equal-L1 diagnostics: (a) both paths advanced the same steps from the
@@ -379,21 +384,21 @@ def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: 
         if w["method"] == "weno":
             kname = "weno_stage_fp64_kernel" if f64 else "weno_stage_mixed_kernel"
         else:
-            # the mixed P=2, 3 stages run two threads per cell (dg_mixed.cu kSingleTpc)
+            # the mixed stage kernel the context's tuner chose (threads per cell)
             kname = ("dg_face_kernel x2 + dg_cell_kernel (one stage)" if f64
-                     else "dg_stage_mixed_pair_kernel" if w["order"] >= 2 else "dg_stage_mixed_kernel")
+                     else DG_MIXED_KERNEL.get(pth["tpc"], "dg_stage_mixed_kernel"))
         if prec == "fp64_fma":
             kname = ("weno_stage_fp64_kernel, FMA-contracted build" if w["method"] == "weno"
                      else "dg_stage_fused_fp64_kernel (one fused FP64 launch per stage, FMA)")
         roofs[prec] = {
             "bound": "fp64" if f64 else "fp32", "achieved": achieved, "peak": pk,
             "unit": "TFLOP/s", "frac": achieved / pk,
-            "traffic": (KERNEL_TRAFFIC_PER_CELL[(name, prec)][0] * cells
-                        if (name, prec) in KERNEL_TRAFFIC_PER_CELL else None),
-            "traffic_source": (KERNEL_TRAFFIC_PER_CELL[(name, prec)][1] + ", scaled by updated cells"
-                               if (name, prec) in KERNEL_TRAFFIC_PER_CELL else None),
+            "traffic": (KERNEL_TRAFFIC_PER_CELL[(name, prec, kname)][0] * cells
+                        if (name, prec, kname) in KERNEL_TRAFFIC_PER_CELL else None),
+            "traffic_source": (KERNEL_TRAFFIC_PER_CELL[(name, prec, kname)][1] + ", scaled by updated cells"
+                               if (name, prec, kname) in KERNEL_TRAFFIC_PER_CELL else None),
             "algorithmic_bytes": hbm_bytes,
-            "kernel": kname, "flops_per_cell_stage": fl,
+            "kernel": kname, "threads_per_cell": pth["tpc"], "flops_per_cell_stage": fl,
             "avg_launch_ms": stage_ms,
             "peak_source": "measured: zk_peak_flops FMA microbenchmark on this GPU "
                            "(MEASURED_PEAKS.json has no FP64/FP32 figure)",

@@ -53,6 +53,11 @@ def test_default_options_and_errors_without_device(lib):
     assert b"method" in lib.zk_last_error()
     assert lib.zk_create(None, C.byref(h)) == 1
     assert lib.zk_version() >= 100
+    # threads per cell of the mixed DG stage: 0 (tuned), 1 or 2
+    lib.zk_default_options(C.byref(o))
+    o.method, o.order, o.tile_tpc = 1, 2, 4
+    assert lib.zk_create(C.byref(o), C.byref(h)) == 1
+    assert b"tile_tpc" in lib.zk_last_error()
 
 
 
