@@ -16,6 +16,7 @@
 // volume quadrature and face integrals by sum factorisation, the Shu-Osher
 // combine and the Persson + Zhang-Shu limiter (src_DG/fluid.cpp:824-992),
 // exchanging what needs all four variables at a point with the partner lane.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -596,14 +597,14 @@ __global__ void __launch_bounds__(NTHREAD, P == 3 ? 1 : 2) dg_stage_fused_fp64_k
 template <int P>
 cudaError_t launch_p(const F64Args& a, cudaStream_t s) {
     constexpr size_t sm = smem_bytes_d<P>();
-    static bool attr_set[64] = {};
+    static std::atomic<bool> attr_set[64];  // per device; any host thread may launch
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (dev >= 0 && dev < 64 && !attr_set[dev].load(std::memory_order_acquire)) {
         const cudaError_t e =
             cudaFuncSetAttribute(dg_stage_fused_fp64_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     const dim3 grid((a.g.nx + TX - 1) / TX, (a.g.ny + TY - 1) / TY);
     dg_stage_fused_fp64_kernel<P><<<grid, NTHREAD, sm, s>>>(a);

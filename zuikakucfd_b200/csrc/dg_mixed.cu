@@ -13,6 +13,7 @@
 // changes.  This file is compiled with --use_fast_math (FP32 division, sqrt,
 // log10 and sin use the MUFU approximations); the combine and limiter
 // arithmetic is rounded explicitly, so both kernels give the same bits.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -1454,14 +1455,14 @@ template <int P, int STAGE, int V>
 cudaError_t batch_one(const DgItem* items, const int* dir, int cap, int grid, cudaStream_t s, int* occ) {
     constexpr size_t sm = smem_bytes<P, dg_variant_rows(V)>();
     constexpr int nt = MTX * dg_variant_rows(V) * dg_variant_tpc(V);
-    static bool attr_set[64] = {};
+    static std::atomic<bool> attr_set[64];  // per device; any host thread may launch
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (dev >= 0 && dev < 64 && !attr_set[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(dg_stage_mixed_batch_kernel<P, STAGE, V>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, dg_stage_mixed_batch_kernel<P, STAGE, V>, nt, sm);
     dg_stage_mixed_batch_kernel<P, STAGE, V><<<grid, nt, sm, s>>>(items, dir, cap);
@@ -1498,13 +1499,13 @@ cudaError_t launch_one(const MixArgs& a, cudaStream_t s) {
     constexpr int rows = pair ? kPairRows : 4, cols = pair ? kPairCols : MTX;
     constexpr size_t sm = pair ? pair_smem_bytes<P, MLP>() : smem_bytes<P, rows>();
     auto* kern = pair ? dg_stage_mixed_pair_kernel<P, TIn, TOut, MLP> : dg_stage_mixed_kernel<P, TIn, TOut>;
-    static bool attr_set[64] = {};
+    static std::atomic<bool> attr_set[64];  // per device; any host thread may launch
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (dev >= 0 && dev < 64 && !attr_set[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
-        attr_set[dev] = true;
+        attr_set[dev].store(true, std::memory_order_release);
     }
     dim3 grid((a.g.nx + cols - 1) / cols, (a.g.ny + rows - 1) / rows);
     kern<<<grid, cols * rows * TPC, sm, s>>>(a);
