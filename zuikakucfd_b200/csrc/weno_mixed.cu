@@ -386,9 +386,10 @@ __device__ __forceinline__ bool stage_tile(const CUtensorMap* tmap, const MixedA
     return true;
 }
 
-// 5 CTAs per SM (40 registers, some spilled; 223 KB of shared memory): the
-// extra resident warps hide more latency than the spills cost (+14% at 4 CTAs
-// and +2.4% more at 5, over 3 CTAs at 72 registers).
+// 5 CTAs per SM (40 registers, 384 bytes spilled; 223 KB of shared memory):
+// the extra resident warps hide more latency than the spills cost.  Per step
+// at 2048^2, same bits: 0.618 ms at 5 CTAs, 0.669 ms at 4 (56 registers, 148
+// bytes spilled), 0.765 ms at 3 (72 registers).
 __global__ void __launch_bounds__(Tile<8>::NTHREAD, 5)
     weno_stage_mixed_kernel(const __grid_constant__ CUtensorMap tmap, MixedArgs a) {
     __shared__ __align__(128) Smem<8> S;
