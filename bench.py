@@ -417,6 +417,7 @@ def measure_single(name: str, args, rank: int, world: int, local: int, pg, e2e: 
                        "parallelism": f"replicas x{world} (independent seeded problems)"},
             "fp64_value": paths["fp64"]["value"], "fp64_fma_value": paths.get("fp64_fma", {}).get("value"),
             "equal_l1": eq,
+            "cell_updates_per_s": hp["value"] / w["dof_per_cell"],
             "speedup_vs_fp64": hp["value"] / paths["fp64"]["value"],
             "speedup_vs_best_fp64": hp["value"] / max(v["value"] for k, v in paths.items() if k != "mixed"),
             "clocks": hp["clocks"], "e2e": e2e_rec,
